@@ -1,0 +1,467 @@
+// Device-resident matrix and PCA plan (layer 2 of the C ABI).
+//
+// The matrix is either copied to HBM once (residency DEVICE) or streamed
+// from host memory in fixed cell chunks through two device buffers on a copy
+// stream, the copy of chunk i+1 overlapping the kernels of chunk i
+// (residency HOST; the reference's out-of-core model, crest/core.py:54-62 and
+// docs/memory_model.md, with device memory bounded by two chunks plus the
+// accumulators).
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "host.cuh"
+
+struct crest_matrix {
+    int device = 0;
+    int64_t n_cells = 0, n_genes = 0, nnz = 0;
+    int residency = CREST_MEM_DEVICE;
+    int64_t chunk_cells = 16384;
+    std::vector<int64_t> h_indptr;
+    const uint32_t *h_indices = nullptr;
+    const float *h_data = nullptr;
+    bool registered = false;
+    crest::DevBuf d_indptr, d_indices, d_data;
+    cudaStream_t compute = nullptr, copy = nullptr;
+    crest::DevBuf buf_idx[2], buf_val[2];
+    cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+    // per-pass staging
+    crest::DevBuf cell_map, gene_map, flag, sub_map, mean, std_, bias;
+    crest::DevBuf out[5];
+};
+
+struct crest_pca {
+    int device = 0;
+    int64_t d = 0, k = 0, n = 0;
+    int precision = CREST_GRAM_BF16X3;
+    crest::DevBuf gram, colsum, vals, vecs, total, shift, xbuf;
+    crest::GramBufs gb;
+    crest::GramWork w;
+    crest_pca_stats stats;
+};
+
+namespace crest {
+namespace {
+
+struct Timer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    cudaStream_t st;
+    explicit Timer(cudaStream_t s) : st(s) {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, st);
+    }
+    double stop() {
+        cudaEventRecord(b, st);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        return ms;
+    }
+    ~Timer() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+
+int bind_device(int dev) {
+    CREST_TRY(require_device());
+    CREST_CUDA_TRY(cudaSetDevice(dev));
+    return CREST_OK;
+}
+
+// Stage cell_map (n_cells) and gene_map (n_genes) of one pass; every mapped
+// row must be < n_rows and every mapped var < n_vars (outputs are sized so).
+int stage_maps(crest_matrix *m, const int64_t *cell_map, const int32_t *gene_map, int64_t n_rows = -1,
+               int64_t n_vars = -1) {
+    CREST_REQUIRE(cell_map && gene_map, CREST_EINVAL, "cell_map / gene_map are NULL");
+    if (n_rows >= 0)
+        for (int64_t i = 0; i < m->n_cells; ++i)
+            CREST_REQUIRE(cell_map[i] < n_rows, CREST_EINVAL, "cell_map holds row %lld but n_rows is %lld",
+                          (long long)cell_map[i], (long long)n_rows);
+    if (n_vars >= 0)
+        for (int64_t i = 0; i < m->n_genes; ++i)
+            CREST_REQUIRE(gene_map[i] < n_vars, CREST_EINVAL, "gene_map holds var %d but n_vars is %lld",
+                          (int)gene_map[i], (long long)n_vars);
+    CREST_TRY(upload(m->cell_map, cell_map, m->n_cells, m->compute));
+    CREST_TRY(upload(m->gene_map, gene_map, m->n_genes, m->compute));
+    return CREST_OK;
+}
+
+DevChunk base_chunk(crest_matrix *m, double target_sum, int log1p) {
+    DevChunk c;
+    c.genes = nullptr;
+    c.values = nullptr;
+    c.span_ptr = m->d_indptr.as<int64_t>();
+    c.span_cell = nullptr;
+    c.base = 0;
+    c.n_spans = 0;
+    c.first_cell = 0;
+    c.cell_map = m->cell_map.as<int64_t>();
+    c.n_cell_map = m->n_cells;
+    c.gene_map = m->gene_map.as<int32_t>();
+    c.n_gene_map = m->n_genes;
+    c.target_sum = target_sum;
+    c.log1p = log1p ? 1 : 0;
+    return c;
+}
+
+// Run fn(chunk) over consecutive cell pieces of at most max_cells cells on
+// the compute stream.  Streaming residency copies each piece's entries into
+// one of two device buffers on the copy stream first.
+template <class F>
+int for_each_piece(crest_matrix *m, const DevChunk &proto, int64_t max_cells, F &&fn) {
+    const int64_t n = m->n_cells;
+    if (m->residency == CREST_MEM_DEVICE) {
+        for (int64_t s0 = 0; s0 < n; s0 += max_cells) {
+            DevChunk c = proto;
+            c.genes = m->d_indices.as<uint32_t>();
+            c.values = m->d_data.as<float>();
+            c.span_ptr = m->d_indptr.as<int64_t>() + s0;
+            c.first_cell = (uint32_t)s0;
+            c.base = 0;
+            c.n_spans = std::min(max_cells, n - s0);
+            CREST_TRY(fn(c));
+        }
+        return CREST_OK;
+    }
+    const int64_t piece = std::min(max_cells, m->chunk_cells);
+    int slot = 0;
+    for (int64_t s0 = 0; s0 < n; s0 += piece, slot ^= 1) {
+        const int64_t s1 = std::min(n, s0 + piece);
+        const int64_t e0 = m->h_indptr[s0], e1 = m->h_indptr[s1];
+        const size_t ne = (size_t)(e1 - e0);
+        CREST_TRY(m->buf_idx[slot].ensure(4 * std::max<size_t>(ne, 1)));
+        CREST_TRY(m->buf_val[slot].ensure(4 * std::max<size_t>(ne, 1)));
+        // the buffer is free once the kernels that read it last have finished
+        CREST_CUDA_TRY(cudaStreamWaitEvent(m->copy, m->ev_free[slot], 0));
+        if (ne) {
+            CREST_CUDA_TRY(cudaMemcpyAsync(m->buf_idx[slot].ptr, m->h_indices + e0, 4 * ne, cudaMemcpyHostToDevice,
+                                           m->copy));
+            CREST_CUDA_TRY(cudaMemcpyAsync(m->buf_val[slot].ptr, m->h_data + e0, 4 * ne, cudaMemcpyHostToDevice,
+                                           m->copy));
+        }
+        CREST_CUDA_TRY(cudaEventRecord(m->ev_ready[slot], m->copy));
+        CREST_CUDA_TRY(cudaStreamWaitEvent(m->compute, m->ev_ready[slot], 0));
+        DevChunk c = proto;
+        c.genes = m->buf_idx[slot].as<uint32_t>();
+        c.values = m->buf_val[slot].as<float>();
+        c.span_ptr = m->d_indptr.as<int64_t>() + s0;
+        c.first_cell = (uint32_t)s0;
+        c.base = e0;
+        c.n_spans = s1 - s0;
+        CREST_TRY(fn(c));
+        CREST_CUDA_TRY(cudaEventRecord(m->ev_free[slot], m->compute));
+    }
+    return CREST_OK;
+}
+
+__global__ void k_init_scores(const double *__restrict__ colsum, const double *__restrict__ V, int64_t d, int64_t k,
+                              double n, double *__restrict__ shift) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= k) return;
+    double s = 0.0;
+    for (int64_t a = 0; a < d; ++a) s += (colsum[a] / n) * V[a * k + j];
+    shift[j] = s;
+}
+
+__global__ void k_fill_scores(const double *__restrict__ shift, int64_t n_rows, int64_t k, float *__restrict__ X) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n_rows * k) return;
+    X[idx] = -__double2float_rn(shift[idx % k]);
+}
+
+}  // namespace
+}  // namespace crest
+
+using namespace crest;
+
+extern "C" {
+
+int crest_matrix_create(crest_matrix **out, const int64_t *indptr, const uint32_t *indices, const float *data,
+                        int64_t n_cells, int64_t n_genes, int32_t residency, int64_t chunk_cells) {
+    CREST_REQUIRE(out, CREST_EINVAL, "out is NULL");
+    *out = nullptr;
+    CREST_REQUIRE(indptr && n_cells >= 0 && n_genes >= 0, CREST_EINVAL, "invalid matrix shape");
+    CREST_REQUIRE(indptr[0] == 0, CREST_EINVAL, "indptr[0] must be 0");
+    for (int64_t i = 0; i < n_cells; ++i)
+        CREST_REQUIRE(indptr[i] <= indptr[i + 1], CREST_EINVAL, "indptr must be non-decreasing");
+    const int64_t nnz = indptr[n_cells];
+    CREST_REQUIRE(nnz == 0 || (indices && data), CREST_EINVAL, "indices / data are NULL");
+    CREST_REQUIRE(residency == CREST_MEM_DEVICE || residency == CREST_MEM_HOST, CREST_EINVAL, "bad residency");
+    CREST_TRY(require_device());
+    crest_matrix *m = new crest_matrix();
+    cudaGetDevice(&m->device);
+    m->n_cells = n_cells;
+    m->n_genes = n_genes;
+    m->nnz = nnz;
+    m->residency = residency;
+    m->chunk_cells = chunk_cells > 0 ? chunk_cells : 16384;
+    m->h_indptr.assign(indptr, indptr + n_cells + 1);
+    auto fail = [&](int rc) {
+        crest_matrix_free(m);
+        return rc;
+    };
+    if (cudaStreamCreateWithFlags(&m->compute, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&m->copy, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error("stream creation failed");
+        return fail(CREST_ECUDA);
+    }
+    for (int i = 0; i < 2; ++i) {
+        cudaEventCreateWithFlags(&m->ev_ready[i], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&m->ev_free[i], cudaEventDisableTiming);
+    }
+    int rc = upload(m->d_indptr, indptr, n_cells + 1, m->compute);
+    if (rc) return fail(rc);
+    if (residency == CREST_MEM_DEVICE) {
+        rc = upload(m->d_indices, indices, nnz, m->compute);
+        if (!rc) rc = upload(m->d_data, data, nnz, m->compute);
+        if (rc) return fail(rc);
+    } else {
+        m->h_indices = indices;
+        m->h_data = data;
+        // pin the caller's buffers when they are not pinned already
+        cudaPointerAttributes at;
+        if (nnz > 0 && cudaPointerGetAttributes(&at, indices) == cudaSuccess && at.type == cudaMemoryTypeUnregistered) {
+            if (cudaHostRegister((void *)indices, 4 * (size_t)nnz, cudaHostRegisterReadOnly) == cudaSuccess &&
+                cudaHostRegister((void *)data, 4 * (size_t)nnz, cudaHostRegisterReadOnly) == cudaSuccess)
+                m->registered = true;
+            cudaGetLastError();
+        }
+        cudaGetLastError();
+    }
+    if (cudaStreamSynchronize(m->compute) != cudaSuccess) {
+        set_error("matrix upload failed: %s", cudaGetErrorString(cudaGetLastError()));
+        return fail(CREST_ECUDA);
+    }
+    *out = m;
+    return CREST_OK;
+}
+
+int crest_matrix_free(crest_matrix *m) {
+    if (!m) return CREST_OK;
+    cudaSetDevice(m->device);
+    if (m->compute) cudaStreamSynchronize(m->compute);
+    if (m->copy) cudaStreamSynchronize(m->copy);
+    if (m->registered) {
+        cudaHostUnregister((void *)m->h_indices);
+        cudaHostUnregister((void *)m->h_data);
+    }
+    m->d_indptr.release();
+    m->d_indices.release();
+    m->d_data.release();
+    for (int i = 0; i < 2; ++i) {
+        m->buf_idx[i].release();
+        m->buf_val[i].release();
+        if (m->ev_ready[i]) cudaEventDestroy(m->ev_ready[i]);
+        if (m->ev_free[i]) cudaEventDestroy(m->ev_free[i]);
+    }
+    for (auto *b : {&m->cell_map, &m->gene_map, &m->flag, &m->sub_map, &m->mean, &m->std_, &m->bias}) b->release();
+    for (auto &b : m->out) b.release();
+    if (m->compute) cudaStreamDestroy(m->compute);
+    if (m->copy) cudaStreamDestroy(m->copy);
+    delete m;
+    return CREST_OK;
+}
+
+int crest_matrix_info(const crest_matrix *m, int64_t *n_cells, int64_t *n_genes, int64_t *nnz) {
+    CREST_REQUIRE(m, CREST_EINVAL, "matrix is NULL");
+    if (n_cells) *n_cells = m->n_cells;
+    if (n_genes) *n_genes = m->n_genes;
+    if (nnz) *nnz = m->nnz;
+    return CREST_OK;
+}
+
+int crest_matrix_qc(crest_matrix *m, const int64_t *cell_map, const int32_t *gene_map, const uint8_t *flag,
+                    int64_t n_rows, int64_t n_vars, double *cell_total, uint32_t *cell_ngenes, double *cell_flag,
+                    uint32_t *gene_ncells, double *gene_total) {
+    CREST_REQUIRE(m, CREST_EINVAL, "matrix is NULL");
+    CREST_TRY(bind_device(m->device));
+    CREST_TRY(stage_maps(m, cell_map, gene_map, n_rows, n_vars));
+    cudaStream_t st = m->compute;
+    CREST_TRY(upload(m->flag, flag, n_vars, st));
+    CREST_TRY(zeros<double>(m->out[0], n_rows, st));
+    CREST_TRY(zeros<uint32_t>(m->out[1], n_rows, st));
+    CREST_TRY(zeros<double>(m->out[2], n_rows, st));
+    CREST_TRY(zeros<uint32_t>(m->out[3], n_vars, st));
+    CREST_TRY(zeros<double>(m->out[4], n_vars, st));
+    RowOut ro{m->out[0].as<double>(), m->out[1].as<uint32_t>(), m->out[2].as<double>()};
+    const DevChunk proto = base_chunk(m, 0.0, 0);
+    CREST_TRY(for_each_piece(m, proto, m->n_cells, [&](const DevChunk &c) {
+        return launch_qc(c, m->flag.as<uint8_t>(), m->out[3].as<uint32_t>(), m->out[4].as<double>(), nullptr, &ro, st);
+    }));
+    if (n_rows) {
+        CREST_CUDA_TRY(cudaMemcpyAsync(cell_total, m->out[0].ptr, 8 * n_rows, cudaMemcpyDeviceToHost, st));
+        CREST_CUDA_TRY(cudaMemcpyAsync(cell_ngenes, m->out[1].ptr, 4 * n_rows, cudaMemcpyDeviceToHost, st));
+        CREST_CUDA_TRY(cudaMemcpyAsync(cell_flag, m->out[2].ptr, 8 * n_rows, cudaMemcpyDeviceToHost, st));
+    }
+    if (n_vars) {
+        CREST_CUDA_TRY(cudaMemcpyAsync(gene_ncells, m->out[3].ptr, 4 * n_vars, cudaMemcpyDeviceToHost, st));
+        CREST_CUDA_TRY(cudaMemcpyAsync(gene_total, m->out[4].ptr, 8 * n_vars, cudaMemcpyDeviceToHost, st));
+    }
+    CREST_CUDA_TRY(cudaStreamSynchronize(st));
+    return CREST_OK;
+}
+
+int crest_matrix_gene_stats(crest_matrix *m, const int64_t *cell_map, const int32_t *gene_map, double target_sum,
+                            int32_t log1p, int64_t n_vars, double *out) {
+    CREST_REQUIRE(m && out, CREST_EINVAL, "NULL argument");
+    CREST_TRY(bind_device(m->device));
+    CREST_TRY(stage_maps(m, cell_map, gene_map, -1, n_vars));
+    cudaStream_t st = m->compute;
+    CREST_TRY(zeros<double>(m->out[0], n_vars * 5, st));
+    const DevChunk proto = base_chunk(m, target_sum, log1p);
+    CREST_TRY(for_each_piece(m, proto, m->n_cells,
+                             [&](const DevChunk &c) { return launch_gene_stats(c, m->out[0].as<double>(), st); }));
+    if (n_vars) CREST_CUDA_TRY(cudaMemcpyAsync(out, m->out[0].ptr, 40 * n_vars, cudaMemcpyDeviceToHost, st));
+    CREST_CUDA_TRY(cudaStreamSynchronize(st));
+    return CREST_OK;
+}
+
+int crest_pca_create(crest_pca **out, int64_t d, int32_t precision) {
+    CREST_REQUIRE(out, CREST_EINVAL, "out is NULL");
+    *out = nullptr;
+    CREST_REQUIRE(d >= 1, CREST_EINVAL, "need at least 1 gene");
+    CREST_REQUIRE(precision >= CREST_GRAM_FP64 && precision <= CREST_GRAM_BF16X3, CREST_EINVAL,
+                  "unknown Gram precision %d", precision);
+    CREST_TRY(require_device());
+    crest_pca *p = new crest_pca();
+    cudaGetDevice(&p->device);
+    p->d = d;
+    p->precision = precision;
+    memset(&p->stats, 0, sizeof p->stats);
+    int rc = zeros<double>(p->gram, d * d, 0);
+    if (!rc) rc = zeros<double>(p->colsum, d, 0);
+    if (!rc) rc = p->gb.ensure(p->w, d, precision, tile_cells_default());
+    if (!rc && cudaDeviceSynchronize() != cudaSuccess) {
+        set_error("PCA plan set-up failed: %s", cudaGetErrorString(cudaGetLastError()));
+        rc = CREST_ECUDA;
+    }
+    if (rc) {
+        crest_pca_free(p);
+        return rc;
+    }
+    *out = p;
+    return CREST_OK;
+}
+
+int crest_pca_free(crest_pca *p) {
+    if (!p) return CREST_OK;
+    cudaSetDevice(p->device);
+    cudaDeviceSynchronize();
+    for (auto *b : {&p->gram, &p->colsum, &p->vals, &p->vecs, &p->total, &p->shift, &p->xbuf}) b->release();
+    p->gb.tile.release();
+    p->gb.colsum_chunk.release();
+    p->gb.n_kept.release();
+    delete p;
+    return CREST_OK;
+}
+
+int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map, const int32_t *gene_map,
+                         double target_sum, int32_t log1p, const int32_t *sub_map, int64_t n_vars,
+                         const crest_scale *scale) {
+    CREST_REQUIRE(p && m, CREST_EINVAL, "NULL plan or matrix");
+    CREST_TRY(bind_device(m->device));
+    for (int64_t i = 0; i < n_vars; ++i)
+        CREST_REQUIRE(sub_map[i] < p->d, CREST_EINVAL, "sub_map must have length n_vars and values < d");
+    cudaStream_t st = m->compute;
+    Timer t(st);
+    CREST_TRY(stage_maps(m, cell_map, gene_map, -1, n_vars));
+    CREST_TRY(upload(m->sub_map, sub_map, n_vars, st));
+    DevScale ds;
+    CREST_TRY(stage_scale(m->mean, m->std_, m->bias, scale, p->d, ds, st));
+    const DevChunk proto = base_chunk(m, target_sum, log1p);
+    CREST_TRY(for_each_piece(m, proto, p->w.m_cap, [&](const DevChunk &c) {
+        return gram_over_chunk(c, m->sub_map.as<int32_t>(), ds, p->w, p->gram.as<double>(), p->colsum.as<double>(), st);
+    }));
+    p->stats.gram_ms = t.stop();
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
+}
+
+int crest_pca_accumulators(crest_pca *p, double **gram_dev, double **colsum_dev) {
+    CREST_REQUIRE(p, CREST_EINVAL, "plan is NULL");
+    if (gram_dev) *gram_dev = p->gram.as<double>();
+    if (colsum_dev) *colsum_dev = p->colsum.as<double>();
+    return CREST_OK;
+}
+
+int crest_pca_solve(crest_pca *p, int64_t n, int64_t k) {
+    CREST_REQUIRE(p, CREST_EINVAL, "plan is NULL");
+    CREST_REQUIRE(n >= 2, CREST_ERUNTIME, "need at least 2 cells and 1 gene");
+    CREST_REQUIRE(k >= 1 && k <= p->d && k <= 128, CREST_EINVAL, "k=%lld must be in [1, min(d, 128)]", (long long)k);
+    CREST_TRY(bind_device(p->device));
+    cudaStream_t st = 0;
+    CREST_TRY(p->vals.ensure(8 * (size_t)k));
+    CREST_TRY(p->vecs.ensure(8 * (size_t)(p->d * k)));
+    CREST_TRY(p->total.ensure(8));
+    CREST_TRY(p->shift.ensure(8 * (size_t)k));
+    Timer t(st);
+    EigStats es{};
+    CREST_TRY(eig_topk(p->gram.as<double>(), p->colsum.as<double>(), p->d, n, k, p->vals.as<double>(),
+                       p->vecs.as<double>(), p->total.as<double>(), &es, st));
+    k_init_scores<<<(unsigned)ceil_div(k, 64), 64, 0, st>>>(p->colsum.as<double>(), p->vecs.as<double>(), p->d, k,
+                                                           (double)n, p->shift.as<double>());
+    CREST_CUDA_TRY(cudaGetLastError());
+    p->stats.solve_ms = t.stop();
+    p->stats.eig_iters = es.iters;
+    p->stats.eig_converged = es.converged;
+    p->stats.eig_residual = es.residual;
+    p->k = k;
+    p->n = n;
+    CREST_REQUIRE(es.converged, CREST_ERUNTIME, "eigensolver did not converge (residual %.3g after %d iterations)",
+                  es.residual, es.iters);
+    return CREST_OK;
+}
+
+int crest_pca_results(crest_pca *p, double *variance, double *loadings, double *total, double *colsum) {
+    CREST_REQUIRE(p, CREST_EINVAL, "plan is NULL");
+    CREST_TRY(bind_device(p->device));
+    if (variance && p->k) CREST_CUDA_TRY(cudaMemcpy(variance, p->vals.ptr, 8 * p->k, cudaMemcpyDeviceToHost));
+    if (loadings && p->k) CREST_CUDA_TRY(cudaMemcpy(loadings, p->vecs.ptr, 8 * p->d * p->k, cudaMemcpyDeviceToHost));
+    if (total) CREST_CUDA_TRY(cudaMemcpy(total, p->total.ptr, 8, cudaMemcpyDeviceToHost));
+    if (colsum) CREST_CUDA_TRY(cudaMemcpy(colsum, p->colsum.ptr, 8 * p->d, cudaMemcpyDeviceToHost));
+    return CREST_OK;
+}
+
+int crest_pca_project(crest_pca *p, crest_matrix *m, const int64_t *cell_map, const int32_t *gene_map,
+                      double target_sum, int32_t log1p, const int32_t *sub_map, int64_t n_vars,
+                      const crest_scale *scale, int64_t n_rows, float *out, int32_t out_mem) {
+    CREST_REQUIRE(p && m && out, CREST_EINVAL, "NULL argument");
+    CREST_REQUIRE(p->k >= 1, CREST_EINVAL, "crest_pca_solve must run before crest_pca_project");
+    CREST_TRY(bind_device(m->device));
+    for (int64_t i = 0; i < n_vars; ++i)
+        CREST_REQUIRE(sub_map[i] < p->d, CREST_EINVAL, "sub_map must have length n_vars and values < d");
+    cudaStream_t st = m->compute;
+    Timer t(st);
+    CREST_TRY(stage_maps(m, cell_map, gene_map, n_rows, n_vars));
+    CREST_TRY(upload(m->sub_map, sub_map, n_vars, st));
+    DevScale ds;
+    CREST_TRY(stage_scale(m->mean, m->std_, m->bias, scale, p->d, ds, st));
+    float *X = out;
+    if (out_mem != CREST_MEM_DEVICE) {
+        CREST_TRY(p->xbuf.ensure(4 * (size_t)std::max<int64_t>(n_rows * p->k, 1)));
+        X = p->xbuf.as<float>();
+    }
+    if (n_rows * p->k)
+        k_fill_scores<<<(unsigned)ceil_div(n_rows * p->k, 256), 256, 0, st>>>(p->shift.as<double>(), n_rows, p->k, X);
+    CREST_CUDA_TRY(cudaGetLastError());
+    const DevChunk proto = base_chunk(m, target_sum, log1p);
+    CREST_TRY(for_each_piece(m, proto, m->n_cells, [&](const DevChunk &c) {
+        return launch_project(c, m->sub_map.as<int32_t>(), ds, p->vecs.as<double>(), (int)p->k, X, 0, st);
+    }));
+    if (out_mem != CREST_MEM_DEVICE && n_rows * p->k)
+        CREST_CUDA_TRY(cudaMemcpyAsync(out, X, 4 * (size_t)(n_rows * p->k), cudaMemcpyDeviceToHost, st));
+    p->stats.project_ms = t.stop();
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
+}
+
+int crest_pca_stats_get(const crest_pca *p, crest_pca_stats *stats) {
+    CREST_REQUIRE(p && stats, CREST_EINVAL, "NULL argument");
+    *stats = p->stats;
+    return CREST_OK;
+}
+
+}  // extern "C"

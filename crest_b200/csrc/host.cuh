@@ -1,0 +1,80 @@
+// Host-side helpers shared by the C ABI translation units.
+#pragma once
+
+#include <stdlib.h>
+
+#include <algorithm>
+
+#include "kernels.cuh"
+
+namespace crest {
+
+inline int require_device() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        set_error("no usable CUDA device (%s); the CREST GPU path has no CPU fallback",
+                  e == cudaSuccess ? "device count is 0" : cudaGetErrorString(e));
+        return CREST_ENODEV;
+    }
+    return CREST_OK;
+}
+
+template <class T>
+inline int upload(DevBuf &b, const T *src, int64_t n, cudaStream_t st) {
+    CREST_TRY(b.ensure(sizeof(T) * (size_t)(n > 0 ? n : 1)));
+    if (n > 0) CREST_CUDA_TRY(cudaMemcpyAsync(b.ptr, src, sizeof(T) * (size_t)n, cudaMemcpyHostToDevice, st));
+    return CREST_OK;
+}
+template <class T>
+inline int zeros(DevBuf &b, int64_t n, cudaStream_t st) {
+    CREST_TRY(b.ensure(sizeof(T) * (size_t)(n > 0 ? n : 1)));
+    CREST_CUDA_TRY(cudaMemsetAsync(b.ptr, 0, sizeof(T) * (size_t)(n > 0 ? n : 1), st));
+    return CREST_OK;
+}
+
+inline int64_t tile_cells_default() {
+    const char *e = getenv("CREST_TILE_CELLS");
+    int64_t v = e ? atoll(e) : 8192;
+    if (v < 64) v = 64;
+    return round_up(v, 64);
+}
+
+// A Gram tile workspace sized for d genes.
+struct GramBufs {
+    DevBuf tile, colsum_chunk, n_kept;
+    int ensure(GramWork &w, int64_t d, int precision, int64_t m_cap) {
+        w.d = d;
+        w.d_pad = round_up(d > 0 ? d : 1, 128);
+        w.m_cap = m_cap;
+        w.precision = precision;
+        CREST_TRY(tile.ensure(gram_tile_bytes(precision, w.d_pad, m_cap)));
+        CREST_TRY(colsum_chunk.ensure(sizeof(double) * (size_t)w.d_pad));
+        CREST_TRY(n_kept.ensure(sizeof(int64_t)));
+        w.tile = tile.ptr;
+        w.colsum_chunk = colsum_chunk.as<double>();
+        w.n_kept = n_kept.as<int64_t>();
+        w.part32 = nullptr;
+        return CREST_OK;
+    }
+};
+
+// Sub-chunk of spans [s0, s0 + n) of a staged chunk.
+inline DevChunk slice(const DevChunk &c, int64_t s0, int64_t n) {
+    DevChunk r = c;
+    r.span_ptr = c.span_ptr + s0;
+    if (c.span_cell) r.span_cell = c.span_cell + s0;
+    else r.first_cell = c.first_cell + (uint32_t)s0;
+    r.n_spans = n;
+    return r;
+}
+
+int gram_over_chunk(const DevChunk &dc, const int32_t *sub_map, const DevScale &ds, GramWork &w, double *gram,
+                    double *colsum, cudaStream_t st);
+
+// Upload mean/std of d genes and derive bias = clip(-mean/std).
+int stage_scale(DevBuf &mean, DevBuf &std_, DevBuf &bias, const crest_scale *t, int64_t d, DevScale &ds,
+                cudaStream_t st);
+
+}  // namespace crest

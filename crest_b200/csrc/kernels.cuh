@@ -1,0 +1,69 @@
+// Launch interfaces of the CREST B200 kernels (host side).
+#pragma once
+
+#include "common.cuh"
+
+namespace crest {
+
+int device_sms();  // SM count of the current device (cached per device)
+
+struct SpanOut {  // per-span QC results (per-chunk API)
+    int64_t *row;
+    double *t;
+    uint32_t *n;
+    double *f;
+};
+struct RowOut {  // per-row QC results added at the cell's row (matrix API)
+    double *t;
+    uint32_t *n;
+    double *f;
+};
+
+int launch_qc(const DevChunk &c, const uint8_t *flag, uint32_t *gene_ncells, double *gene_total,
+              const SpanOut *span, const RowOut *row, cudaStream_t st);
+int launch_gene_stats(const DevChunk &c, double *out, cudaStream_t st);
+// out row index: the cell's row, or the span index when by_span != 0
+int launch_project(const DevChunk &c, const int32_t *sub_map, const DevScale &t, const double *V, int k,
+                   float *out, int by_span, cudaStream_t st);
+int launch_scale_bias(const double *mean, const double *std, double mv, int64_t d, double *bias, cudaStream_t st);
+
+// ------------------------------------------------------------------ Gram
+// One Gram tile job: the chunk's kept cells become the K dimension of a
+// dense, gene-major tile T[d_pad][m_pad] (cells contiguous) that holds the
+// scaled matrix restricted to the HVG columns.  FP64 keeps S itself (zero
+// where nothing is stored) so the SYRK reproduces the reference's sums;
+// FP32/BF16x3 hold Z = S - shift (shift = -bias, i.e. the dense scaled
+// matrix), which keeps the reduced-precision products centred.
+struct GramWork {
+    int64_t d, d_pad;
+    int64_t m_cap;          // max cells per tile (multiple of 64)
+    int precision;
+    void *tile;             // FP64: double; FP32: float; BF16X3: hi then lo (bf16)
+    double *colsum_chunk;   // [d] FP64 column sums of S for the current tile
+    int64_t *n_kept;        // [1] kept cells in the current tile
+    float *part32;          // [d_pad * d_pad] FP32 partial (FP32 / BF16X3)
+};
+
+size_t gram_tile_bytes(int precision, int64_t d_pad, int64_t m_cap);
+// Densify spans [0, c.n_spans) of a chunk (n_spans <= m_cap) into the tile
+// and accumulate its colsum / kept count.
+int launch_densify(const DevChunk &c, const int32_t *sub_map, const DevScale &t, const GramWork &w,
+                   cudaStream_t st);
+// gram (d x d row-major, upper triangle) += T T^T of the current tile; adds
+// colsum_chunk to colsum.
+int launch_syrk_fold(const GramWork &w, int64_t m, const DevScale &t, double *gram, double *colsum,
+                     cudaStream_t st);
+
+// ------------------------------------------------------------ eigensolver
+struct EigStats {
+    int iters;
+    int converged;
+    double residual;
+};
+// cov = (G - c c^T / n) / (n - 1) from the upper triangle of G; top-k
+// eigenpairs (descending, clamped at 0; largest |loading| positive) and
+// trace.  vals [k], vecs [d x k] row-major, total [1]: device pointers.
+int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_t k, double *vals, double *vecs,
+             double *total, EigStats *stats, cudaStream_t st);
+
+}  // namespace crest

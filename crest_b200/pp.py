@@ -1,0 +1,240 @@
+"""Preprocessing on :class:`~crest_b200.core.BioFrame` (the reference's
+``crest.pp``, crest/pp.py): QC metrics and filters, lazy ``normalize_total`` /
+``log1p`` / ``scale``, per-gene statistics and seurat / cell_ranger highly
+variable genes.
+
+The count passes run on the GPU: CSR stores through the device-resident
+whole-matrix entry points, triplet stores chunk by chunk through the
+drop-in native functions (:mod:`crest_b200._native`).  The per-gene HVG math
+is O(n_vars) numpy on the host, with the reference's formulas.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+import pandas as pd
+
+from . import _lib, _native
+from .core import BioFrame
+
+__all__ = ["calculate_qc_metrics", "filter_cells", "filter_genes", "normalize_total", "log1p", "scale",
+           "gene_stats", "highly_variable_genes"]
+
+
+# --------------------------------------------------------------------------- QC
+def _mito_flag(bf: BioFrame, mito_prefix: Optional[str]) -> np.ndarray:
+    p = mito_prefix.upper() if mito_prefix else None
+    return np.array([bool(p) and n.upper().startswith(p) for n in bf.var_names], dtype=bool)
+
+
+def _qc_sums(bf: BioFrame, flag: np.ndarray):
+    ct = np.zeros(bf.n_obs, np.float64)
+    cn = np.zeros(bf.n_obs, np.uint32)
+    cf = np.zeros(bf.n_obs, np.float64)
+    gn = np.zeros(bf.n_vars, np.uint32)
+    gt = np.zeros(bf.n_vars, np.float64)
+    dm = bf.device_matrix()
+    if dm is not None:
+        cmap, gmap = bf._cell_map(), bf._gene_map()
+        f = np.ascontiguousarray(flag, dtype=np.bool_)
+        _lib.call("crest_matrix_qc", dm.handle, _lib.ptr(cmap), _lib.ptr(gmap), _lib.ptr(f), bf.n_obs, bf.n_vars,
+                  _lib.ptr(ct), _lib.ptr(cn), _lib.ptr(cf), _lib.ptr(gn), _lib.ptr(gt))
+    else:
+        for ctx in bf.iter_ctx(transform=False):
+            _native.qc(*ctx, flag, ct, cn, cf, gn, gt)
+    return ct, cn, cf, gn, gt
+
+
+def calculate_qc_metrics(bf: BioFrame, mito_prefix: Optional[str] = "MT-", inplace: bool = True):
+    """Per-cell ``total_counts``, ``n_genes_by_counts``, ``pct_counts_mt`` and per-gene
+    ``n_cells_by_counts``, ``total_counts`` on the raw counts of kept cells/genes
+    (crest/pp.py:25-45)."""
+    ct, cn, cf, gn, gt = _qc_sums(bf, _mito_flag(bf, mito_prefix))
+    pct = np.divide(cf, ct, out=np.zeros_like(ct), where=ct > 0) * 100.0
+    obs = pd.DataFrame({"n_genes_by_counts": cn.astype(np.int64), "total_counts": ct, "pct_counts_mt": pct})
+    var = pd.DataFrame({"n_cells_by_counts": gn.astype(np.int64), "total_counts": gt})
+    if not inplace:
+        return obs, var
+    for c in obs.columns:
+        bf.obs[c] = obs[c].to_numpy()
+    for c in var.columns:
+        bf.var[c] = var[c].to_numpy()
+    return None
+
+
+def filter_cells(bf: BioFrame, min_genes: Optional[int] = None, min_counts: Optional[float] = None,
+                 max_genes: Optional[int] = None, max_counts: Optional[float] = None,
+                 max_pct_mt: Optional[float] = None) -> BioFrame:
+    """New BioFrame keeping cells within the thresholds (crest/pp.py:48-65)."""
+    obs, _ = calculate_qc_metrics(bf, inplace=False)
+    keep = np.ones(bf.n_obs, bool)
+    ng, tc, mt = (obs["n_genes_by_counts"].to_numpy(), obs["total_counts"].to_numpy(),
+                  obs["pct_counts_mt"].to_numpy())
+    if min_genes is not None:
+        keep &= ng >= min_genes
+    if max_genes is not None:
+        keep &= ng <= max_genes
+    if min_counts is not None:
+        keep &= tc >= min_counts
+    if max_counts is not None:
+        keep &= tc <= max_counts
+    if max_pct_mt is not None:
+        keep &= mt <= max_pct_mt
+    return bf._subset(obs_mask=keep)
+
+
+def filter_genes(bf: BioFrame, min_cells: Optional[int] = None, min_counts: Optional[float] = None,
+                 max_cells: Optional[int] = None, max_counts: Optional[float] = None) -> BioFrame:
+    """New BioFrame keeping genes within the thresholds, counted over kept cells (crest/pp.py:68-82)."""
+    _, var = calculate_qc_metrics(bf, inplace=False)
+    keep = np.ones(bf.n_vars, bool)
+    nc, tc = var["n_cells_by_counts"].to_numpy(), var["total_counts"].to_numpy()
+    if min_cells is not None:
+        keep &= nc >= min_cells
+    if max_cells is not None:
+        keep &= nc <= max_cells
+    if min_counts is not None:
+        keep &= tc >= min_counts
+    if max_counts is not None:
+        keep &= tc <= max_counts
+    return bf._subset(var_mask=keep)
+
+
+# --------------------------------------------------------------------------- lazy transforms
+def normalize_total(bf: BioFrame, target_sum: float = 1e4) -> BioFrame:
+    """Scale each cell to ``target_sum`` total counts, applied lazily (crest/pp.py:86-93)."""
+    if target_sum is None or target_sum <= 0:
+        raise ValueError("target_sum must be positive")
+    if any(op[0] == "log1p" for op in bf.ops):
+        raise ValueError("normalize_total must come before log1p")
+    bf.ops = [op for op in bf.ops if op[0] != "normalize_total"] + [("normalize_total", float(target_sum))]
+    return bf
+
+
+def log1p(bf: BioFrame) -> BioFrame:
+    """Natural log(1 + x), applied lazily."""
+    if not any(op[0] == "log1p" for op in bf.ops):
+        bf.ops.append(("log1p",))
+    return bf
+
+
+def scale(bf: BioFrame, max_value: Optional[float] = 10.0) -> BioFrame:
+    """Record ``sc.pp.scale(max_value)`` for :func:`crest_b200.tl.pca`, which applies it exactly
+    without densifying the matrix (crest/pp.py:103-111)."""
+    bf.uns["scale"] = {"max_value": float(max_value) if max_value else 0.0}
+    return bf
+
+
+# --------------------------------------------------------------------------- gene statistics / HVG
+def gene_stats(bf: BioFrame) -> np.ndarray:
+    """(n_vars, 5): sum x, sum x^2, sum expm1(x), sum expm1(x)^2, nnz of the transformed matrix."""
+    out = np.zeros((bf.n_vars, 5), np.float64)
+    dm = bf.device_matrix()
+    if dm is not None:
+        cmap, gmap = bf._cell_map(), bf._gene_map()
+        target, log = bf._transform()
+        _lib.call("crest_matrix_gene_stats", dm.handle, _lib.ptr(cmap), _lib.ptr(gmap), float(target), int(log),
+                  bf.n_vars, _lib.ptr(out))
+    else:
+        for ctx in bf.iter_ctx():
+            _native.gene_stats(*ctx, out)
+    return out
+
+
+def _mean_var(s1: np.ndarray, s2: np.ndarray, n: int):
+    """Mean and ddof=1 variance from sums (crest/pp.py:123-126), clamped at 0."""
+    mean = s1 / n
+    var = (s2 - n * mean * mean) / (n - 1) if n > 1 else np.zeros_like(mean)
+    return mean, np.maximum(var, 0.0)
+
+
+def _cut_codes(x: np.ndarray, n_bins: int) -> np.ndarray:
+    """Bin index of each value under ``pandas.cut(x, n_bins)``: equal-width, right-closed
+    bins, the lowest edge pushed down by 0.1% of the range (crest/pp.py:129-136)."""
+    lo, hi = float(np.min(x)), float(np.max(x))
+    if lo == hi:
+        return np.zeros(len(x), np.int64)
+    edges = np.linspace(lo, hi, n_bins + 1)
+    edges[0] -= (hi - lo) * 0.001
+    return np.clip(np.searchsorted(edges, x, side="left") - 1, 0, n_bins - 1)
+
+
+def highly_variable_genes(bf: BioFrame, n_top_genes: Optional[int] = None, flavor: str = "seurat",
+                          n_bins: int = 20, min_mean: float = 0.0125, max_mean: float = 3.0,
+                          min_disp: float = 0.5, max_disp: float = np.inf, subset: bool = False,
+                          batch_key: Optional[str] = None) -> BioFrame:
+    """``sc.pp.highly_variable_genes`` for ``flavor="seurat"`` (log-normalised data) and
+    ``"cell_ranger"`` (crest/pp.py:201-292).  Adds var columns ``means``, ``dispersions``,
+    ``dispersions_norm``, ``highly_variable``, ``mean_log``, ``std_log``, ``n_cells_expr``
+    and records the ops the log-scale mean/std were computed under (for ``tl.pca``)."""
+    if flavor in ("seurat_v3", "seurat_v3_paper"):
+        raise NotImplementedError("flavor='seurat_v3' is outside this package's hot path")
+    if batch_key is not None:
+        raise NotImplementedError("batch_key is supported for flavor='seurat_v3' only")
+    n = bf.n_obs
+    st = gene_stats(bf)
+    mean_log, var_log = _mean_var(st[:, 0], st[:, 1], n)
+    if flavor == "seurat":
+        mean, var = _mean_var(st[:, 2], st[:, 3], n)
+    elif flavor == "cell_ranger":
+        mean, var = mean_log.copy(), var_log.copy()
+    else:
+        raise ValueError('flavor must be "seurat" or "cell_ranger"')
+    mean = mean.copy()
+    mean[mean == 0] = 1e-12
+    with np.errstate(divide="ignore", invalid="ignore"):
+        disp = var / mean
+    if flavor == "seurat":
+        disp[disp == 0] = np.nan
+        with np.errstate(divide="ignore"):
+            disp = np.log(disp)
+        mean = np.log1p(mean)
+        codes = _cut_codes(mean, n_bins)
+        nb = n_bins
+    else:
+        edges = np.r_[-np.inf, np.percentile(mean, np.arange(10, 105, 5)), np.inf]
+        codes = np.clip(np.searchsorted(edges, mean, side="left") - 1, 0, len(edges) - 2)
+        nb = len(edges) - 1
+
+    centre = np.full(nb, np.nan)
+    spread = np.full(nb, np.nan)
+    for b in range(nb):
+        vals = disp[(codes == b) & ~np.isnan(disp)]
+        if flavor == "seurat":
+            if len(vals):
+                centre[b] = vals.mean()
+            if len(vals) > 1:
+                spread[b] = vals.std(ddof=1)
+        elif len(vals):
+            med = np.median(vals)
+            centre[b] = med
+            spread[b] = np.median(np.abs(vals - med)) / 0.6744897501960817  # MAD, normal-consistent
+    if flavor == "seurat":  # single-gene bins get a normalised dispersion of 1
+        single = np.isnan(spread)
+        spread[single] = centre[single]
+        centre[single] = 0.0
+    with np.errstate(divide="ignore", invalid="ignore"):
+        disp_norm = (disp - centre[codes]) / spread[codes]
+
+    if n_top_genes is not None:
+        ok = disp_norm[~np.isnan(disp_norm)]
+        k = min(n_top_genes, ok.size, bf.n_vars)
+        cutoff = np.sort(ok)[::-1][k - 1]
+        hv = np.nan_to_num(disp_norm, nan=-np.inf) >= cutoff
+    else:
+        dn = np.nan_to_num(disp_norm)
+        hv = (mean > min_mean) & (mean < max_mean) & (dn > min_disp) & (dn < max_disp)
+
+    std_log = np.sqrt(var_log)
+    std_log[std_log == 0] = 1.0
+    cols = {"means": mean, "dispersions": disp, "dispersions_norm": disp_norm, "highly_variable": hv,
+            "mean_log": mean_log, "std_log": std_log, "n_cells_expr": st[:, 4].astype(np.int64)}
+    for name, v in cols.items():
+        bf.var[name] = v
+    bf.uns["hvg"] = {"flavor": flavor, "ops": list(bf.ops)}
+    if subset:
+        return bf._subset(var_mask=hv)
+    return bf

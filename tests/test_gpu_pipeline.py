@@ -1,0 +1,116 @@
+"""End-to-end GPU pipeline (crest_b200.pp / crest_b200.tl) against golden
+vectors from the reference's own Python orchestration (tests/golden), and
+invariance checks: chunking, store kind, residency, Gram precision.
+
+Parity bar: QC integers and the kept sets bit-exact, the HVG set identical,
+dispersions_norm within 1e-6, max principal angle <= 0.01 degree against the
+FP64 reference, scores within 1e-4 relative after sign alignment."""
+
+import os
+
+import numpy as np
+import pandas as pd
+import pytest
+
+import crest_b200 as cb
+from oracle import pipeline as op
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def load_case(name):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(HERE, "golden", "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg.CASES[name], mg.case_input(name), dict(np.load(os.path.join(HERE, "golden", f"{name}.npz")))
+
+
+def frame(inp, residency="device", chunk_nnz=None):
+    indptr, indices, data, n_genes, names = inp
+    bf = cb.BioFrame.from_csr(indptr, indices, data, n_genes, var=pd.DataFrame({"gene_name": names}))
+    bf.store.residency = residency
+    bf.store.chunk_cells = 700
+    if chunk_nnz:
+        bf.chunk_nnz = chunk_nnz
+    return bf
+
+
+def pipeline(bf, c, precision="bf16x3"):
+    bf = cb.pp.filter_cells(bf, min_genes=c["min_genes"])
+    bf = cb.pp.filter_genes(bf, min_cells=c["min_cells"])
+    cb.pp.normalize_total(bf, 1e4)
+    cb.pp.log1p(bf)
+    cb.pp.highly_variable_genes(bf, n_top_genes=c["n_top"])
+    cb.pp.scale(bf, max_value=10)
+    cb.tl.pca(bf, n_comps=c["n_comps"], gram_precision=precision)
+    return bf
+
+
+def max_angle(A, B):
+    return float(op.principal_angles_deg(A, B).max())
+
+
+def aligned_rel_err(X, R):
+    X = X.astype(np.float64)
+    R = R.astype(np.float64)
+    s = np.sign((X * R).sum(0))
+    s[s == 0] = 1
+    return float(np.max(np.linalg.norm(X * s - R, axis=0) / np.linalg.norm(R, axis=0)))
+
+
+@pytest.mark.parametrize("name", ["small", "pbmc3k_like"])
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "bf16x3"])
+def test_pipeline_matches_reference_golden(name, precision):
+    c, inp, g = load_case(name)
+    bf = frame(inp)
+    obs0, var0 = cb.pp.calculate_qc_metrics(bf, inplace=False)
+    assert np.array_equal(obs0["n_genes_by_counts"].to_numpy(), g["qc_n_genes_by_counts"])
+    assert np.array_equal(obs0["total_counts"].to_numpy(), g["qc_total_counts"])
+    assert np.array_equal(obs0["pct_counts_mt"].to_numpy(), g["qc_pct_counts_mt"])
+    assert np.array_equal(var0["n_cells_by_counts"].to_numpy(), g["qc_gene_n_cells"])
+    assert np.array_equal(var0["total_counts"].to_numpy(), g["qc_gene_total"])
+    bf = pipeline(bf, c, precision)
+    assert np.array_equal(bf.obs["cell_id"].to_numpy(), g["kept_cells"])
+    assert np.array_equal(bf.var["gene_id"].to_numpy(), g["kept_genes"])
+    assert np.array_equal(bf.var["highly_variable"].to_numpy(), g["highly_variable"])
+    dn, gdn = bf.var["dispersions_norm"].to_numpy(), g["dispersions_norm"]
+    assert np.array_equal(np.isnan(dn), np.isnan(gdn))
+    ok = ~np.isnan(gdn)
+    assert np.max(np.abs(dn[ok] - gdn[ok])) <= 1e-6
+    np.testing.assert_allclose(bf.var["mean_log"].to_numpy(), g["mean_log"], rtol=1e-12)
+    var_tol = {"fp64": 1e-9, "fp32": 1e-5, "bf16x3": 1e-4}[precision]
+    np.testing.assert_allclose(bf.uns["pca"]["variance"], g["variance"], rtol=var_tol)
+    X = bf.obsm["X_pca"]
+    R = g["X_pca"]
+    assert max_angle(X[: len(R)], R) <= 0.01
+    assert aligned_rel_err(X[: len(R)], R) <= 1e-4
+
+
+def test_chunking_store_and_residency_invariance():
+    c, inp, g = load_case("small")
+    a = pipeline(frame(inp), c, "fp64")
+    b = pipeline(frame(inp, residency="host"), c, "fp64")
+    assert np.array_equal(a.obsm["X_pca"], b.obsm["X_pca"])
+    indptr, indices, data, n_genes, names = inp
+    cells = np.repeat(np.arange(len(indptr) - 1), np.diff(indptr)).astype(np.uint32)
+    t = cb.BioFrame.from_triplets(cells, indices, data, len(indptr) - 1, n_genes,
+                                  var=pd.DataFrame({"gene_name": names}))
+    t.chunk_nnz = 20_000
+    tt = pipeline(t, c, "fp64")
+    assert np.array_equal(tt.var["highly_variable"].to_numpy(), a.var["highly_variable"].to_numpy())
+    assert max_angle(tt.obsm["X_pca"], a.obsm["X_pca"]) <= 1e-6
+    assert aligned_rel_err(tt.obsm["X_pca"], a.obsm["X_pca"]) <= 1e-5
+
+
+def test_precision_forms_against_fp64():
+    c, inp, g = load_case("pbmc3k_like")
+    ref = pipeline(frame(inp), c, "fp64")
+    for prec in ("fp32", "bf16x3"):
+        got = pipeline(frame(inp), c, prec)
+        L0 = ref.uns["pca"]["projection"]["loadings"]
+        L1 = got.uns["pca"]["projection"]["loadings"]
+        assert float(op.subspace_angles_deg(L0, L1).max()) <= 0.01
+        assert aligned_rel_err(got.obsm["X_pca"], ref.obsm["X_pca"]) <= 1e-4
