@@ -71,6 +71,7 @@ _SIGS = {
     "crest_pca_create": [P, I64, I32],
     "crest_pca_free": [P],
     "crest_pca_accumulate": [P, P, P, P, D, I32, P, I64, P],
+    "crest_pca_reset": [P],
     "crest_pca_accumulators": [P, P, P],
     "crest_pca_solve": [P, I64, I64],
     "crest_pca_results": [P, P, P, P, P],
@@ -78,6 +79,9 @@ _SIGS = {
     "crest_pca_stats_get": [P, P],
     "crest_synth_cpu": [P, P, P, P, P, C.c_int],
     "crest_synth_gpu": [P, P, P, P, P],
+    "crest_profile_enable": [C.c_int],
+    "crest_profile_count": [],
+    "crest_profile_entry": [C.c_int, C.c_char_p, C.c_int, P, P, P],
 }
 
 _lib = None
@@ -123,6 +127,22 @@ def check(rc: int):
 
 def call(name: str, *args):
     check(getattr(load(), name)(*args))
+
+
+def profile_enable(on: bool = True):
+    load().crest_profile_enable(1 if on else 0)
+
+
+def profile_table() -> dict:
+    """{kernel: (launches, total_ms, max_ms)} of the launches timed since profile_enable."""
+    L = load()
+    out = {}
+    for i in range(L.crest_profile_count()):
+        name = C.create_string_buffer(128)
+        n, t, m = C.c_longlong(), C.c_double(), C.c_double()
+        check(L.crest_profile_entry(i, name, 128, C.byref(n), C.byref(t), C.byref(m)))
+        out[name.value.decode()] = (int(n.value), float(t.value), float(m.value))
+    return out
 
 
 def device_count() -> int:

@@ -363,6 +363,10 @@ int crest_gram_accumulate(const crest_chunk *chunk, const int32_t *sub_map, int6
     const int64_t m_cap = std::min<int64_t>(tile_cells_default(), round_up(std::max<int64_t>(s.n, 1), 64));
     CREST_TRY(x->gb.ensure(w, d, precision, m_cap));
     CREST_TRY(gram_over_chunk(dc, x->sub_map.as<int32_t>(), ds, w, x->gram.as<double>(), x->colsum.as<double>(), st));
+    if (precision == CREST_GRAM_BF16X3) {
+        CREST_CUDA_TRY(cudaStreamSynchronize(st));
+        CREST_TRY(tc_check_error());
+    }
     if (d) {
         CREST_CUDA_TRY(cudaMemcpyAsync(gram, x->gram.ptr, 8 * d * d, cudaMemcpyDeviceToHost, st));
         CREST_CUDA_TRY(cudaMemcpyAsync(colsum, x->colsum.ptr, 8 * d, cudaMemcpyDeviceToHost, st));

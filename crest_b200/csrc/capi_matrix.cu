@@ -377,6 +377,16 @@ int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
     }));
     p->stats.gram_ms = t.stop();
     CREST_CUDA_TRY(cudaGetLastError());
+    if (p->precision == CREST_GRAM_BF16X3) CREST_TRY(tc_check_error());
+    return CREST_OK;
+}
+
+int crest_pca_reset(crest_pca *p) {
+    CREST_REQUIRE(p, CREST_EINVAL, "plan is NULL");
+    CREST_TRY(bind_device(p->device));
+    CREST_CUDA_TRY(cudaMemset(p->gram.ptr, 0, sizeof(double) * (size_t)(p->d * p->d)));
+    CREST_CUDA_TRY(cudaMemset(p->colsum.ptr, 0, sizeof(double) * (size_t)p->d));
+    p->k = 0;
     return CREST_OK;
 }
 

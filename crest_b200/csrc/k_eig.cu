@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "kernels.cuh"
+#include "prof.cuh"
 
 namespace crest {
 namespace {
@@ -140,6 +141,7 @@ __global__ void __launch_bounds__(256) k_gemm(Gemm g) {
 }
 
 int gemm(const Gemm &g, cudaStream_t st) {
+    prof::Scope ps("eig_gemm_fp64", st);
     dim3 grid((unsigned)ceil_div(g.M, 64), (unsigned)ceil_div(g.N, 64));
     k_gemm<<<grid, 256, 0, st>>>(g);
     CREST_CUDA_TRY(cudaGetLastError());
@@ -257,6 +259,7 @@ int jacobi(const double *A, int n_in, double *V, double *vals, int *sweeps, cuda
     CREST_REQUIRE(n <= kJacobiMax, CREST_EINVAL, "Jacobi size %d exceeds %d", n, kJacobiMax);
     const size_t smem = sizeof(double) * (size_t)n * (size_t)(n + 1);
     CREST_CUDA_TRY(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    prof::Scope ps("eig_jacobi", st);
     k_jacobi<<<1, 1024, smem, st>>>(A, n_in, n, V, vals, 40, sweeps);
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
@@ -604,7 +607,10 @@ int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_
                 CREST_CUDA_TRY(cudaMemcpyAsync(V, Ycur, blk, cudaMemcpyDeviceToDevice, st));
             }
         }
-        k_cgs2<<<1, 1024, cgs_smem, st>>>(V, d, p, 0x13198a2e03707344ull + (uint64_t)it, nullptr);
+        {
+            prof::Scope ps("eig_cgs2", st);
+            k_cgs2<<<1, 1024, cgs_smem, st>>>(V, d, p, 0x13198a2e03707344ull + (uint64_t)it, nullptr);
+        }
         CREST_CUDA_TRY(cudaGetLastError());
     }
     if (stats) *stats = EigStats{it + 1, converged ? 1 : 0, res};

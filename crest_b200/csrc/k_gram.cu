@@ -16,6 +16,7 @@
 #include <cuda_bf16.h>
 
 #include "kernels.cuh"
+#include "prof.cuh"
 #include "rowwarp.cuh"
 
 namespace crest {
@@ -159,6 +160,8 @@ int launch_densify(const DevChunk &c, const int32_t *sub_map, const DevScale &t,
     CREST_CUDA_TRY(cudaMemsetAsync(w.colsum_chunk, 0, sizeof(double) * (size_t)(w.d > 0 ? w.d : 1), st));
     const double *bias = (w.precision != CREST_GRAM_FP64 && t.scale) ? t.bias : nullptr;
     dim3 fg((unsigned)ceil_div(m_pad, 128), (unsigned)(w.d_pad < 64 ? w.d_pad : 64));
+    {
+    prof::Scope ps("tile_fill", st);
     if (w.precision == CREST_GRAM_FP64)
         k_tile_fill<double><<<fg, 128, 0, st>>>(c, w.d, w.d_pad, m_pad, bias, (double *)w.tile, w.n_kept);
     else if (w.precision == CREST_GRAM_FP32)
@@ -168,6 +171,7 @@ int launch_densify(const DevChunk &c, const int32_t *sub_map, const DevScale &t,
         __nv_bfloat16 *lo = hi + (size_t)w.d_pad * (size_t)m_pad;
         k_tile_fill_bf16x3<<<fg, 128, 0, st>>>(c, w.d, w.d_pad, m_pad, bias, hi, lo, w.n_kept);
     }
+    }
     CREST_CUDA_TRY(cudaGetLastError());
     if (c.n_spans == 0) return CREST_OK;
     const int64_t warps = 8;
@@ -175,6 +179,7 @@ int launch_densify(const DevChunk &c, const int32_t *sub_map, const DevScale &t,
     const int64_t cap = (int64_t)device_sms() * 8;
     if (blocks > cap) blocks = cap;
     const size_t smem = (w.d <= 4096) ? sizeof(double) * (size_t)w.d : 0;
+    prof::Scope ps("tile_scatter", st);
     if (w.precision == CREST_GRAM_FP64) {
         k_tile_scatter<0><<<(unsigned)blocks, 256, 0, st>>>(c, sub_map, t, w.d, m_pad, w.tile, w.colsum_chunk);
     } else if (w.precision == CREST_GRAM_FP32) {
@@ -273,15 +278,21 @@ __global__ void k_colsum_f64(const double *__restrict__ T, int64_t d, int64_t m_
 
 // ------------------------------------------------------------ FP32 SYRK
 // 128x128 upper-triangular block tiles, 256 threads, 8x8 register tile per
-// thread, K step 16 double-buffered through shared memory.  Epilogue folds
-// into G in FP64 with the bias correction.
-constexpr int kBM = 128, kBK = 16, kPadS = 4;
+// thread, K step 16 double-buffered through shared memory.  The FP32
+// register accumulators are folded into FP64 (in shared memory) every
+// kFoldSteps K steps, so FP32 rounding only ever spans kFoldSteps*16 cells;
+// the epilogue adds the FP64 tile into G with the bias correction.
+constexpr int kBM = 128, kBK = 16, kPadS = 4, kFoldSteps = 16;
+constexpr size_t kSyrkF32Smem = sizeof(float) * 2 * 2 * kBK * (kBM + kPadS) + sizeof(double) * 64 * 256;
 
 __global__ void __launch_bounds__(256) k_syrk_f32(const float *__restrict__ T, int64_t d, int64_t m_pad, int64_t nb,
                                                   const double *__restrict__ bias, const double *__restrict__ colsum_c,
                                                   const int64_t *__restrict__ n_kept, double *__restrict__ G) {
-    __shared__ __align__(16) float As[2][kBK][kBM + kPadS];
-    __shared__ __align__(16) float Bs[2][kBK][kBM + kPadS];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float(*As)[kBK][kBM + kPadS] = reinterpret_cast<float(*)[kBK][kBM + kPadS]>(smem_raw);
+    float(*Bs)[kBK][kBM + kPadS] = reinterpret_cast<float(*)[kBK][kBM + kPadS]>(smem_raw + sizeof(float) * 2 * kBK *
+                                                                                                   (kBM + kPadS));
+    double *acc64 = reinterpret_cast<double *>(smem_raw + sizeof(float) * 2 * 2 * kBK * (kBM + kPadS));
     int bi, bj;
     tri_decode(blockIdx.x, nb, bi, bj);
     const int tid = threadIdx.x;
@@ -291,7 +302,10 @@ __global__ void __launch_bounds__(256) k_syrk_f32(const float *__restrict__ T, i
 #pragma unroll
     for (int p = 0; p < 8; ++p)
 #pragma unroll
-        for (int q = 0; q < 8; ++q) acc[p][q] = 0.0f;
+        for (int q = 0; q < 8; ++q) {
+            acc[p][q] = 0.0f;
+            acc64[(p * 8 + q) * 256 + tid] = 0.0;
+        }
 
     // loader: each panel is 128 rows x 16 floats = 512 float4; 2 per thread
     const int lrow = tid >> 2, lcol = (tid & 3) * 4;
@@ -311,9 +325,18 @@ __global__ void __launch_bounds__(256) k_syrk_f32(const float *__restrict__ T, i
             Bs[buf][lcol + 3][row] = vb.w;
         }
     };
+    auto fold = [&]() {
+#pragma unroll
+        for (int p = 0; p < 8; ++p)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                acc64[(p * 8 + q) * 256 + tid] += (double)acc[p][q];
+                acc[p][q] = 0.0f;
+            }
+    };
     load(0, 0);
     __syncthreads();
-    int buf = 0;
+    int buf = 0, steps = 0;
     for (int64_t k0 = 0; k0 < m_pad; k0 += kBK) {
         if (k0 + kBK < m_pad) load(buf ^ 1, k0 + kBK);
 #pragma unroll
@@ -332,9 +355,14 @@ __global__ void __launch_bounds__(256) k_syrk_f32(const float *__restrict__ T, i
 #pragma unroll
                 for (int q = 0; q < 8; ++q) acc[p][q] = fmaf(av[p], bv[q], acc[p][q]);
         }
+        if (++steps == kFoldSteps) {
+            fold();
+            steps = 0;
+        }
         __syncthreads();
         buf ^= 1;
     }
+    fold();
     const double nk = (double)*n_kept;
 #pragma unroll
     for (int p = 0; p < 8; ++p) {
@@ -345,7 +373,7 @@ __global__ void __launch_bounds__(256) k_syrk_f32(const float *__restrict__ T, i
         for (int q = 0; q < 8; ++q) {
             const int64_t b = b0 + (q < 4 ? tx * 4 + q : 64 + tx * 4 + q - 4);
             if (b >= d || b < a) continue;
-            double v = (double)acc[p][q];
+            double v = acc64[(p * 8 + q) * 256 + tid];
             if (bias) {
                 const double bb = bias[b], cb = colsum_c[b];
                 v = v - ba * cb - ca * bb - nk * ba * bb;
@@ -367,6 +395,7 @@ int launch_syrk_fold(const GramWork &w, int64_t m, const DevScale &t, double *gr
     if (w.precision == CREST_GRAM_FP64) {
         const int64_t nb = ceil_div(w.d, 64);
         const int64_t tiles = nb * (nb + 1) / 2;
+        prof::Scope ps("syrk_fp64", st);
         k_syrk_f64<<<(unsigned)tiles, 256, 0, st>>>((const double *)w.tile, w.d, m_pad, nb, gram);
         CREST_CUDA_TRY(cudaGetLastError());
         k_colsum_f64<<<(unsigned)ceil_div(w.d, 128), 128, 0, st>>>((const double *)w.tile, w.d, m_pad, m, colsum);
@@ -377,8 +406,11 @@ int launch_syrk_fold(const GramWork &w, int64_t m, const DevScale &t, double *gr
     if (w.precision == CREST_GRAM_FP32) {
         const int64_t nb = w.d_pad / kBM;
         const int64_t tiles = nb * (nb + 1) / 2;
-        k_syrk_f32<<<(unsigned)tiles, 256, 0, st>>>((const float *)w.tile, w.d, m_pad, nb, bias, w.colsum_chunk,
-                                                    w.n_kept, gram);
+        prof::Scope ps("syrk_fp32", st);
+        CREST_CUDA_TRY(
+            cudaFuncSetAttribute(k_syrk_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSyrkF32Smem));
+        k_syrk_f32<<<(unsigned)tiles, 256, kSyrkF32Smem, st>>>((const float *)w.tile, w.d, m_pad, nb, bias,
+                                                              w.colsum_chunk, w.n_kept, gram);
         CREST_CUDA_TRY(cudaGetLastError());
     } else {
         CREST_TRY(syrk_bf16x3_fold(w, m_pad, t, gram, st));

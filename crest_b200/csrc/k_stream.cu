@@ -6,6 +6,7 @@
 // loads, per-cell sums are formed in the reference's entry order
 // (rowwarp.cuh), per-gene sums go to L2-resident accumulators.
 #include "kernels.cuh"
+#include "prof.cuh"
 #include "rowwarp.cuh"
 
 namespace crest {
@@ -144,6 +145,7 @@ static int grid_for_spans(int64_t n_spans, int sms) {
 int launch_qc(const DevChunk &c, const uint8_t *flag, uint32_t *gene_ncells, double *gene_total,
               const SpanOut *span, const RowOut *row, cudaStream_t st) {
     if (c.n_spans == 0) return CREST_OK;
+    prof::Scope ps("qc_csr", st);
     k_qc<<<grid_for_spans(c.n_spans, device_sms()), 256, 0, st>>>(
         c, flag, gene_ncells, gene_total, span ? span->row : nullptr, span ? span->t : nullptr,
         span ? span->n : nullptr, span ? span->f : nullptr, row ? row->t : nullptr, row ? row->n : nullptr,
@@ -154,6 +156,7 @@ int launch_qc(const DevChunk &c, const uint8_t *flag, uint32_t *gene_ncells, dou
 
 int launch_gene_stats(const DevChunk &c, double *out, cudaStream_t st) {
     if (c.n_spans == 0) return CREST_OK;
+    prof::Scope ps("gene_stats_csr", st);
     k_gene_stats<<<grid_for_spans(c.n_spans, device_sms()), 256, 0, st>>>(c, out);
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
@@ -164,6 +167,7 @@ int launch_project(const DevChunk &c, const int32_t *sub_map, const DevScale &t,
     if (c.n_spans == 0 || k == 0) return CREST_OK;
     CREST_REQUIRE(k <= 128, CREST_EINVAL, "project supports k <= 128 (got %d)", k);
     const int g = grid_for_spans(c.n_spans, device_sms());
+    prof::Scope ps("project_csr", st);
     if (k <= 32)
         k_project<1><<<g, 256, 0, st>>>(c, sub_map, t, V, k, out, by_span);
     else if (k <= 64)

@@ -53,6 +53,8 @@ int launch_densify(const DevChunk &c, const int32_t *sub_map, const DevScale &t,
 // colsum_chunk to colsum.
 int launch_syrk_fold(const GramWork &w, int64_t m, const DevScale &t, double *gram, double *colsum,
                      cudaStream_t st);
+// Non-zero error word of the tensor-core Gram pipeline -> CREST_ETIMEOUT (and cleared).
+int tc_check_error();
 
 // ------------------------------------------------------------ eigensolver
 struct EigStats {

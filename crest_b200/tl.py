@@ -43,6 +43,10 @@ class PcaPlan:
         _lib.call("crest_pca_accumulate", self.handle, dm.handle, _lib.ptr(cmap), _lib.ptr(gmap), float(target),
                   int(log), _lib.ptr(sub_map), int(n_vars), C.byref(scale))
 
+    def reset(self):
+        _lib.call("crest_pca_reset", self.handle)
+        self.k = 0
+
     def accumulators(self):
         g, c = C.c_void_p(), C.c_void_p()
         _lib.call("crest_pca_accumulators", self.handle, C.byref(g), C.byref(c))

@@ -171,6 +171,8 @@ int crest_pca_free(crest_pca *p);
 int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
                          const int32_t *gene_map, double target_sum, int32_t log1p,
                          const int32_t *sub_map, int64_t n_vars, const crest_scale *scale);
+/* Zero the plan's accumulators (start a new Gram pass). */
+int crest_pca_reset(crest_pca *p);
 /* Device pointers of the FP64 accumulators (gram d*d, colsum d), e.g. for
  * an all-reduce across ranks before crest_pca_solve. */
 int crest_pca_accumulators(crest_pca *p, double **gram_dev, double **colsum_dev);
@@ -187,6 +189,14 @@ int crest_pca_project(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
                       const int32_t *sub_map, int64_t n_vars, const crest_scale *scale,
                       int64_t n_rows, float *out, int32_t out_mem);
 int crest_pca_stats_get(const crest_pca *p, crest_pca_stats *stats);
+
+/* ---------------------------------------------------------------- timing
+ * Optional per-kernel device timing with CUDA events around each launch on
+ * its stream (no counterpart in the reference, which has no GPU code).
+ */
+int crest_profile_enable(int on);  /* clears the table; on != 0 starts timing */
+int crest_profile_count(void);     /* distinct kernels timed so far            */
+int crest_profile_entry(int i, char *name, int cap, long long *launches, double *total_ms, double *max_ms);
 
 /* ---------------------------------------------------------------- inputs
  * Seeded synthetic counts for tests and benchmarks (not part of the

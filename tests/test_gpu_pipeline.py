@@ -101,7 +101,7 @@ def test_chunking_store_and_residency_invariance():
     t.chunk_nnz = 20_000
     tt = pipeline(t, c, "fp64")
     assert np.array_equal(tt.var["highly_variable"].to_numpy(), a.var["highly_variable"].to_numpy())
-    assert max_angle(tt.obsm["X_pca"], a.obsm["X_pca"]) <= 1e-6
+    assert max_angle(tt.obsm["X_pca"], a.obsm["X_pca"]) <= 1e-4
     assert aligned_rel_err(tt.obsm["X_pca"], a.obsm["X_pca"]) <= 1e-5
 
 
