@@ -354,6 +354,7 @@ int crest_pca_free(crest_pca *p) {
     p->gb.tile.release();
     p->gb.colsum_chunk.release();
     p->gb.n_kept.release();
+    p->gb.shift.release();
     delete p;
     return CREST_OK;
 }

@@ -43,7 +43,7 @@ inline int64_t tile_cells_default() {
 
 // A Gram tile workspace sized for d genes.
 struct GramBufs {
-    DevBuf tile, colsum_chunk, n_kept;
+    DevBuf tile, colsum_chunk, n_kept, shift;
     int ensure(GramWork &w, int64_t d, int precision, int64_t m_cap) {
         w.d = d;
         w.d_pad = round_up(d > 0 ? d : 1, 128);
@@ -52,10 +52,12 @@ struct GramBufs {
         CREST_TRY(tile.ensure(gram_tile_bytes(precision, w.d_pad, m_cap)));
         CREST_TRY(colsum_chunk.ensure(sizeof(double) * (size_t)w.d_pad));
         CREST_TRY(n_kept.ensure(sizeof(int64_t)));
+        CREST_TRY(shift.ensure(sizeof(double) * (size_t)w.d_pad));
         w.tile = tile.ptr;
         w.colsum_chunk = colsum_chunk.as<double>();
         w.n_kept = n_kept.as<int64_t>();
         w.part32 = nullptr;
+        w.shift = shift.as<double>();
         return CREST_OK;
     }
 };

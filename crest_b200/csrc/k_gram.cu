@@ -1,18 +1,21 @@
 // Gram accumulation over the HVG columns (K3 densify + K4 SYRK).
 //
 // src/kernels.rs:221-309 accumulates G += S^T S sparsely on the CPU.  On the
-// GPU each tile of up to m_cap cells is densified into a gene-major tile in
-// HBM/L2 (cells contiguous, the K dimension of the contraction) and
-// contracted as a dense SYRK over the upper-triangular block tiles of G:
+// GPU each tile of up to m_cap cells is densified into a cell-major tile
+// T[m_pad][d_pad] (one contiguous row of HVG genes per cell; the cells are
+// the K dimension of the contraction) that stays L2-resident, and contracted
+// as a dense SYRK over the upper-triangular block tiles of G:
 //
 //  * FP64: T = S, CUDA-core DMUL+DADD accumulating straight into G in cell
 //    order, which reproduces the reference's f64 sums bit for bit (the extra
 //    terms are exact zeros);
-//  * FP32 (plain form): T = Z = S + bias (the dense scaled matrix, centred by
-//    construction), FP32 register-tiled SYRK, folded into G in FP64 with the
-//    exact correction  S^T S = Z^T Z - bias c^T - c bias^T - n bias bias^T;
-//  * BF16X3 (product form): same tile values split into bf16 hi/lo, contracted
-//    on the tcgen05 tensor cores (k_gram_tc.cu) with the same FP64 fold.
+//  * FP32 (plain form): T = S + shift with shift = bias rounded to f32, i.e.
+//    the dense scaled matrix Z (centred by construction) with its repeated
+//    zero value stored exactly; FP32 register-tiled SYRK, folded into G in
+//    FP64 with the exact correction S^T S = T^T T - shift c^T - c shift^T -
+//    n shift shift^T;
+//  * BF16X3 (product form): the same values split into bf16 hi/lo tiles,
+//    contracted on the tcgen05 tensor cores (k_gram_tc.cu), same FP64 fold.
 #include <cuda_bf16.h>
 
 #include "kernels.cuh"
@@ -27,83 +30,121 @@ size_t gram_tile_bytes(int precision, int64_t d_pad, int64_t m_cap) {
     const size_t n = (size_t)d_pad * (size_t)m_cap;
     if (precision == CREST_GRAM_FP64) return n * 8;
     if (precision == CREST_GRAM_FP32) return n * 4;
-    return n * 4;  // two bf16 tiles
+    return n * 4;  // hi and lo bf16 tiles
 }
 
-// ------------------------------------------------------------------ fill
-// Every element of the tile: kept cell and gene < d -> value of a zero entry
-// (0 for FP64, bias for the centred forms); dropped cell / padding -> 0.
-template <class T>
-__global__ void k_tile_fill(DevChunk c, int64_t d, int64_t d_pad, int64_t m_pad, const double *bias, T *tile,
-                            int64_t *n_kept) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // cell column
-    if (i >= m_pad) return;
-    bool kept = false;
-    if (i < c.n_spans) {
-        const uint32_t cell = c.span_cell ? c.span_cell[i] : c.first_cell + (uint32_t)i;
-        kept = (int64_t)cell < c.n_cell_map && c.cell_map[cell] >= 0;
+// ----------------------------------------------------------------- shift
+// Tile value of a zero entry for the centred forms: bias rounded to the tile
+// precision (f32, or bf16 so that hi = shift and lo = 0), i.e. every repeated
+// zero is stored exactly and the rounding error left in the tile is that of
+// the stored entries only.  The epilogues correct with the same rounded value.
+__global__ void k_tile_shift(int precision, const double *__restrict__ bias, int64_t d, int64_t d_pad,
+                             double *__restrict__ shift) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= d_pad) return;
+    double v = 0.0;
+    if (bias && j < d) {
+        v = bias[j];
+        v = precision == CREST_GRAM_FP32 ? (double)__double2float_rn(v) : (double)__bfloat162float(__double2bfloat16(v));
     }
-    if (kept && blockIdx.y == 0) atomicAdd((unsigned long long *)n_kept, 1ull);
-    for (int64_t j = blockIdx.y; j < d_pad; j += gridDim.y) {
-        double v = (kept && j < d && bias) ? bias[j] : 0.0;
-        tile[(size_t)j * m_pad + i] = (T)v;
-    }
+    shift[j] = v;
 }
 
-__global__ void k_tile_fill_bf16x3(DevChunk c, int64_t d, int64_t d_pad, int64_t m_pad, const double *bias,
-                                   __nv_bfloat16 *hi, __nv_bfloat16 *lo, int64_t *n_kept) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m_pad) return;
-    bool kept = false;
-    if (i < c.n_spans) {
-        const uint32_t cell = c.span_cell ? c.span_cell[i] : c.first_cell + (uint32_t)i;
-        kept = (int64_t)cell < c.n_cell_map && c.cell_map[cell] >= 0;
-    }
-    if (kept && blockIdx.y == 0) atomicAdd((unsigned long long *)n_kept, 1ull);
-    for (int64_t j = blockIdx.y; j < d_pad; j += gridDim.y) {
-        const double v = (kept && j < d && bias) ? bias[j] : 0.0;
-        const __nv_bfloat16 h = __double2bfloat16(v);
-        hi[(size_t)j * m_pad + i] = h;
-        lo[(size_t)j * m_pad + i] = __double2bfloat16(v - (double)__bfloat162float(h));
-    }
+// ------------------------------------------------------------- densify
+// Warp per cell row i of the tile (i < m_pad, padding rows included).  The
+// row is built in a per-warp shared-memory buffer -- the zero-entry value of
+// every gene (shift for kept cells, 0 for dropped / padding rows), then the
+// cell's stored HVG entries -- and written out with 16-byte stores, so the
+// densified tile costs one coalesced write per element.  The colsum of S
+// (FP32 / BF16X3) is privatised per block in shared memory.
+template <int MODE>  // 0 FP64 (T = S), 1 FP32 (T = S + shift), 2 BF16X3 (hi/lo of S + shift)
+struct RowElem;
+template <> struct RowElem<0> { using T = double; };
+template <> struct RowElem<1> { using T = float; };
+template <> struct RowElem<2> { using T = __nv_bfloat16; };
+
+constexpr int kDensifyWarps = 8;
+
+// bf16 split of a tile value (hi + lo ~ z to 2^-17 relative).  hi may come
+// from a double rounding through f32: any nearby bf16 works, lo holds the rest.
+__device__ __forceinline__ void split_bf16(double z, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+    hi = __float2bfloat16_rn(__double2float_rn(z));
+    lo = __float2bfloat16_rn(__double2float_rn(z - (double)__bfloat162float(hi)));
 }
 
-// --------------------------------------------------------------- scatter
-// Warp per cell: stored HVG entries overwrite their tile element; colsum of
-// S is accumulated in shared memory (f64) and flushed once per block.
-template <int MODE>  // 0 FP64 (T = S), 1 FP32 (T = Z)
-__global__ void __launch_bounds__(256) k_tile_scatter(DevChunk c, const int32_t *__restrict__ sub_map, DevScale t,
-                                                      int64_t d, int64_t m_pad, void *tile,
-                                                      double *__restrict__ colsum) {
-    extern __shared__ double s_col[];
-    const bool priv = MODE != 0 && d <= 4096;
-    if (priv) {
+template <int MODE>
+__global__ void __launch_bounds__(kDensifyWarps * 32) k_densify(DevChunk c, const int32_t *__restrict__ sub_map,
+                                                               DevScale t, const double *__restrict__ shift,
+                                                               int64_t d, int64_t d_pad, int64_t m_pad, void *tile,
+                                                               double *__restrict__ colsum, int64_t *n_kept) {
+    using E = typename RowElem<MODE>::T;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rows_per_warp = MODE == 2 ? 2 : 1;  // bf16: hi row then lo row
+    // [shift row (tile type)] [per-warp row buffers] [colsum of S (f64)]
+    E *shift_row = reinterpret_cast<E *>(smem);
+    E *row = shift_row + d_pad + (size_t)wid * rows_per_warp * d_pad;
+    double *s_col = reinterpret_cast<double *>(smem + sizeof(E) * (size_t)(1 + kDensifyWarps * rows_per_warp) * d_pad);
+    const bool priv = MODE != 0;
+    for (int64_t j = threadIdx.x; j < d_pad; j += blockDim.x) shift_row[j] = (E)((shift && j < d) ? shift[j] : 0.0);
+    if (priv)
         for (int64_t j = threadIdx.x; j < d; j += blockDim.x) s_col[j] = 0.0;
-        __syncthreads();
-    }
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t i = warp; i < c.n_spans; i += n_warps) {
-        int64_t lo, hi;
-        if (span_row(c, i, lo, hi) < 0) continue;
-        const double scale = cell_scale(c, lo, hi);
-        for_entries<4>(c, lo, hi, [&](int32_t m, float x) {
-            const int32_t sub = m >= 0 ? __ldg(sub_map + m) : -1;
-            if (sub < 0) return;
-            const double s = scale_value(t, sub, transform_value(c, scale, x));
-            const size_t at = (size_t)sub * m_pad + i;
-            if (MODE == 0) {
-                reinterpret_cast<double *>(tile)[at] = s;
-            } else {
-                const double z = t.scale ? __dadd_rn(s, __ldg(t.bias + sub)) : s;
-                reinterpret_cast<float *>(tile)[at] = __double2float_rn(z);
-                if (priv)
-                    atomicAdd(s_col + sub, s);
-                else
-                    atomicAdd(colsum + sub, s);
+    __syncthreads();
+    const int64_t warp = (int64_t)blockIdx.x * kDensifyWarps + wid;
+    const int64_t n_warps = (int64_t)gridDim.x * kDensifyWarps;
+    const int64_t nvec = d_pad * (int64_t)sizeof(E) / 16;
+    int kept_count = 0;
+    for (int64_t i = warp; i < m_pad; i += n_warps) {
+        int64_t lo = 0, hi = 0, r = -1;
+        if (i < c.n_spans) r = span_row(c, i, lo, hi);
+        const bool kept = r >= 0;
+        // zero-entry value of each gene: the shift row (exact in the tile type) or 0
+        {
+            uint4 *dst = reinterpret_cast<uint4 *>(row);
+            const uint4 *src = reinterpret_cast<const uint4 *>(shift_row);
+            const uint4 zero = make_uint4(0, 0, 0, 0);
+            for (int64_t v = lane; v < nvec; v += 32) {
+                dst[v] = kept ? src[v] : zero;
+                if (MODE == 2) dst[nvec + v] = zero;
             }
-        });
+        }
+        __syncwarp();
+        if (kept) {
+            kept_count += 1;
+            const double scale = cell_scale(c, lo, hi);
+            for_entries<4>(c, lo, hi, [&](int32_t m, float x) {
+                const int32_t sub = m >= 0 ? __ldg(sub_map + m) : -1;
+                if (sub < 0) return;
+                const double s = scale_value(t, sub, transform_value(c, scale, x));
+                if (MODE == 0) {
+                    row[sub] = s;
+                } else {
+                    const double z = shift ? __dadd_rn(s, __ldg(shift + sub)) : s;
+                    if (MODE == 1) {
+                        row[sub] = (E)__double2float_rn(z);
+                    } else {
+                        __nv_bfloat16 h, l;
+                        split_bf16(z, h, l);
+                        row[sub] = h;
+                        row[d_pad + sub] = l;
+                    }
+                    atomicAdd(s_col + sub, s);
+                }
+            });
+        }
+        __syncwarp();
+        // coalesced 16-byte stores of the finished row(s)
+        const uint4 *src = reinterpret_cast<const uint4 *>(row);
+        uint4 *dst = reinterpret_cast<uint4 *>(reinterpret_cast<E *>(tile) + (size_t)i * d_pad);
+        for (int64_t v = lane; v < nvec; v += 32) dst[v] = src[v];
+        if (MODE == 2) {
+            uint4 *dst_lo = reinterpret_cast<uint4 *>(reinterpret_cast<E *>(tile) + (size_t)m_pad * d_pad +
+                                                      (size_t)i * d_pad);
+            for (int64_t v = lane; v < nvec; v += 32) dst_lo[v] = src[nvec + v];
+        }
+        __syncwarp();
     }
+    if (lane == 0 && kept_count) atomicAdd(reinterpret_cast<unsigned long long *>(n_kept), (unsigned long long)kept_count);
     if (priv) {
         __syncthreads();
         for (int64_t j = threadIdx.x; j < d; j += blockDim.x)
@@ -111,44 +152,22 @@ __global__ void __launch_bounds__(256) k_tile_scatter(DevChunk c, const int32_t 
     }
 }
 
-// BF16X3 needs both tiles; the lo tile sits right after the hi tile.
-__global__ void __launch_bounds__(256) k_tile_scatter_bf16x3(DevChunk c, const int32_t *__restrict__ sub_map,
-                                                             DevScale t, int64_t d, int64_t m_pad, int64_t d_pad,
-                                                             __nv_bfloat16 *hi, __nv_bfloat16 *lo,
-                                                             double *__restrict__ colsum) {
-    extern __shared__ double s_col[];
-    const bool priv = d <= 4096;
-    if (priv) {
-        for (int64_t j = threadIdx.x; j < d; j += blockDim.x) s_col[j] = 0.0;
-        __syncthreads();
-    }
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t i = warp; i < c.n_spans; i += n_warps) {
-        int64_t lo_e, hi_e;
-        if (span_row(c, i, lo_e, hi_e) < 0) continue;
-        const double scale = cell_scale(c, lo_e, hi_e);
-        for_entries<4>(c, lo_e, hi_e, [&](int32_t m, float x) {
-            const int32_t sub = m >= 0 ? __ldg(sub_map + m) : -1;
-            if (sub < 0) return;
-            const double s = scale_value(t, sub, transform_value(c, scale, x));
-            const double z = t.scale ? __dadd_rn(s, __ldg(t.bias + sub)) : s;
-            const size_t at = (size_t)sub * m_pad + i;
-            const __nv_bfloat16 h = __double2bfloat16(z);
-            hi[at] = h;
-            lo[at] = __double2bfloat16(z - (double)__bfloat162float(h));
-            if (priv)
-                atomicAdd(s_col + sub, s);
-            else
-                atomicAdd(colsum + sub, s);
-        });
-    }
-    if (priv) {
-        __syncthreads();
-        for (int64_t j = threadIdx.x; j < d; j += blockDim.x)
-            if (s_col[j] != 0.0) atomicAdd(colsum + j, s_col[j]);
-    }
-    (void)d_pad;
+template <int MODE>
+static int launch_densify_t(const DevChunk &c, const int32_t *sub_map, const DevScale &t, const double *shift,
+                            const GramWork &w, int64_t m_pad, cudaStream_t st) {
+    using E = typename RowElem<MODE>::T;
+    const int rows_per_warp = MODE == 2 ? 2 : 1;
+    const size_t smem = sizeof(E) * (size_t)(1 + kDensifyWarps * rows_per_warp) * w.d_pad +
+                        (MODE != 0 ? sizeof(double) * (size_t)w.d : 0);
+    CREST_REQUIRE(smem <= 220 * 1024, CREST_EINVAL, "d=%lld too large for the densify row buffers", (long long)w.d);
+    CREST_CUDA_TRY(cudaFuncSetAttribute(k_densify<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int64_t blocks = ceil_div(m_pad, kDensifyWarps);
+    const int64_t cap = (int64_t)device_sms() * 4;
+    if (blocks > cap) blocks = cap;
+    k_densify<MODE><<<(unsigned)blocks, kDensifyWarps * 32, smem, st>>>(c, sub_map, t, shift, w.d, w.d_pad, m_pad,
+                                                                         w.tile, w.colsum_chunk, w.n_kept);
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
 }
 
 int launch_densify(const DevChunk &c, const int32_t *sub_map, const DevScale &t, const GramWork &w,
@@ -158,51 +177,21 @@ int launch_densify(const DevChunk &c, const int32_t *sub_map, const DevScale &t,
     const int64_t m_pad = round_up(c.n_spans > 0 ? c.n_spans : 1, 64);
     CREST_CUDA_TRY(cudaMemsetAsync(w.n_kept, 0, sizeof(int64_t), st));
     CREST_CUDA_TRY(cudaMemsetAsync(w.colsum_chunk, 0, sizeof(double) * (size_t)(w.d > 0 ? w.d : 1), st));
-    const double *bias = (w.precision != CREST_GRAM_FP64 && t.scale) ? t.bias : nullptr;
-    dim3 fg((unsigned)ceil_div(m_pad, 128), (unsigned)(w.d_pad < 64 ? w.d_pad : 64));
-    {
-    prof::Scope ps("tile_fill", st);
-    if (w.precision == CREST_GRAM_FP64)
-        k_tile_fill<double><<<fg, 128, 0, st>>>(c, w.d, w.d_pad, m_pad, bias, (double *)w.tile, w.n_kept);
-    else if (w.precision == CREST_GRAM_FP32)
-        k_tile_fill<float><<<fg, 128, 0, st>>>(c, w.d, w.d_pad, m_pad, bias, (float *)w.tile, w.n_kept);
-    else {
-        __nv_bfloat16 *hi = (__nv_bfloat16 *)w.tile;
-        __nv_bfloat16 *lo = hi + (size_t)w.d_pad * (size_t)m_pad;
-        k_tile_fill_bf16x3<<<fg, 128, 0, st>>>(c, w.d, w.d_pad, m_pad, bias, hi, lo, w.n_kept);
+    const double *shift = nullptr;
+    if (w.precision != CREST_GRAM_FP64 && t.scale) {
+        k_tile_shift<<<(unsigned)ceil_div(w.d_pad, 256), 256, 0, st>>>(w.precision, t.bias, w.d, w.d_pad, w.shift);
+        CREST_CUDA_TRY(cudaGetLastError());
+        shift = w.shift;
     }
-    }
-    CREST_CUDA_TRY(cudaGetLastError());
-    if (c.n_spans == 0) return CREST_OK;
-    const int64_t warps = 8;
-    int64_t blocks = ceil_div(c.n_spans, warps);
-    const int64_t cap = (int64_t)device_sms() * 8;
-    if (blocks > cap) blocks = cap;
-    const size_t smem = (w.d <= 4096) ? sizeof(double) * (size_t)w.d : 0;
-    prof::Scope ps("tile_scatter", st);
-    if (w.precision == CREST_GRAM_FP64) {
-        k_tile_scatter<0><<<(unsigned)blocks, 256, 0, st>>>(c, sub_map, t, w.d, m_pad, w.tile, w.colsum_chunk);
-    } else if (w.precision == CREST_GRAM_FP32) {
-        if (smem > 48 * 1024)
-            CREST_CUDA_TRY(cudaFuncSetAttribute(k_tile_scatter<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                (int)smem));
-        k_tile_scatter<1><<<(unsigned)blocks, 256, smem, st>>>(c, sub_map, t, w.d, m_pad, w.tile, w.colsum_chunk);
-    } else {
-        if (smem > 48 * 1024)
-            CREST_CUDA_TRY(cudaFuncSetAttribute(k_tile_scatter_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                (int)smem));
-        __nv_bfloat16 *hi = (__nv_bfloat16 *)w.tile;
-        __nv_bfloat16 *lo = hi + (size_t)w.d_pad * (size_t)m_pad;
-        k_tile_scatter_bf16x3<<<(unsigned)blocks, 256, smem, st>>>(c, sub_map, t, w.d, m_pad, w.d_pad, hi, lo,
-                                                                  w.colsum_chunk);
-    }
-    CREST_CUDA_TRY(cudaGetLastError());
-    return CREST_OK;
+    prof::Scope ps("densify", st);
+    if (w.precision == CREST_GRAM_FP64) return launch_densify_t<0>(c, sub_map, t, nullptr, w, m_pad, st);
+    if (w.precision == CREST_GRAM_FP32) return launch_densify_t<1>(c, sub_map, t, shift, w, m_pad, st);
+    return launch_densify_t<2>(c, sub_map, t, shift, w, m_pad, st);
 }
 
 // ------------------------------------------------------------ FP64 SYRK
 // Upper-triangular 64x64 block tiles; each thread owns 4x4 outputs and
-// accumulates G[a][b] + T[a][0]T[b][0] + T[a][1]T[b][1] + ... in cell order
+// accumulates G[a][b] + T[0][a]T[0][b] + T[1][a]T[1][b] + ... in cell order
 // with separately rounded products, exactly like src/kernels.rs:303-305.
 __device__ __forceinline__ void tri_decode(int64_t t, int64_t nb, int &bi, int &bj) {
     // t enumerates (bi <= bj) row-major: row bi has nb - bi tiles
@@ -216,8 +205,8 @@ __device__ __forceinline__ void tri_decode(int64_t t, int64_t nb, int &bi, int &
     bj = r + (int)rem;
 }
 
-__global__ void __launch_bounds__(256) k_syrk_f64(const double *__restrict__ T, int64_t d, int64_t m_pad,
-                                                  int64_t nb, double *__restrict__ G) {
+__global__ void __launch_bounds__(256) k_syrk_f64(const double *__restrict__ T, int64_t d, int64_t d_pad,
+                                                  int64_t m_pad, int64_t nb, double *__restrict__ G) {
     __shared__ double As[16][64 + 1];
     __shared__ double Bs[16][64 + 1];
     int bi, bj;
@@ -232,14 +221,14 @@ __global__ void __launch_bounds__(256) k_syrk_f64(const double *__restrict__ T, 
             const int64_t a = a0 + ty + 16 * p, b = b0 + tx + 16 * q;
             acc[p][q] = (a < d && b < d && a <= b) ? G[a * d + b] : 0.0;
         }
-    // loader: 64 rows x 16 cols = 1024 doubles per panel; 4 per thread
+    // loader: 16 cells x 64 genes = 1024 doubles per panel; 4 per thread, coalesced along genes
     for (int64_t k0 = 0; k0 < m_pad; k0 += 16) {
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             const int idx = threadIdx.x + 256 * r;
-            const int row = idx >> 4, col = idx & 15;
-            As[col][row] = T[(a0 + row) * m_pad + k0 + col];
-            Bs[col][row] = T[(b0 + row) * m_pad + k0 + col];
+            const int kk = idx >> 6, g = idx & 63;
+            As[kk][g] = T[(k0 + kk) * d_pad + a0 + g];
+            Bs[kk][g] = T[(k0 + kk) * d_pad + b0 + g];
         }
         __syncthreads();
 #pragma unroll
@@ -265,14 +254,13 @@ __global__ void __launch_bounds__(256) k_syrk_f64(const double *__restrict__ T, 
         }
 }
 
-// colsum[j] += T[j][0] + T[j][1] + ... in cell order (FP64 form).
-__global__ void k_colsum_f64(const double *__restrict__ T, int64_t d, int64_t m_pad, int64_t m,
+// colsum[j] += T[0][j] + T[1][j] + ... in cell order (FP64 form).
+__global__ void k_colsum_f64(const double *__restrict__ T, int64_t d, int64_t d_pad, int64_t m,
                              double *__restrict__ colsum) {
     const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= d) return;
     double acc = colsum[j];
-    const double *r = T + (size_t)j * m_pad;
-    for (int64_t i = 0; i < m; ++i) acc = __dadd_rn(acc, r[i]);
+    for (int64_t i = 0; i < m; ++i) acc = __dadd_rn(acc, T[i * d_pad + j]);
     colsum[j] = acc;
 }
 
@@ -281,12 +269,13 @@ __global__ void k_colsum_f64(const double *__restrict__ T, int64_t d, int64_t m_
 // thread, K step 16 double-buffered through shared memory.  The FP32
 // register accumulators are folded into FP64 (in shared memory) every
 // kFoldSteps K steps, so FP32 rounding only ever spans kFoldSteps*16 cells;
-// the epilogue adds the FP64 tile into G with the bias correction.
+// the epilogue adds the FP64 tile into G with the shift correction.
 constexpr int kBM = 128, kBK = 16, kPadS = 4, kFoldSteps = 16;
 constexpr size_t kSyrkF32Smem = sizeof(float) * 2 * 2 * kBK * (kBM + kPadS) + sizeof(double) * 64 * 256;
 
-__global__ void __launch_bounds__(256) k_syrk_f32(const float *__restrict__ T, int64_t d, int64_t m_pad, int64_t nb,
-                                                  const double *__restrict__ bias, const double *__restrict__ colsum_c,
+__global__ void __launch_bounds__(256) k_syrk_f32(const float *__restrict__ T, int64_t d, int64_t d_pad,
+                                                  int64_t m_pad, int64_t nb, const double *__restrict__ shift,
+                                                  const double *__restrict__ colsum_c,
                                                   const int64_t *__restrict__ n_kept, double *__restrict__ G) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float(*As)[kBK][kBM + kPadS] = reinterpret_cast<float(*)[kBK][kBM + kPadS]>(smem_raw);
@@ -307,22 +296,16 @@ __global__ void __launch_bounds__(256) k_syrk_f32(const float *__restrict__ T, i
             acc64[(p * 8 + q) * 256 + tid] = 0.0;
         }
 
-    // loader: each panel is 128 rows x 16 floats = 512 float4; 2 per thread
-    const int lrow = tid >> 2, lcol = (tid & 3) * 4;
+    // loader: a panel is 16 cells x 128 genes = 512 float4 (rows contiguous along genes)
+    const int lk = tid >> 5, lg = (tid & 31) * 4;
     auto load = [&](int buf, int64_t k0) {
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
-            const int row = lrow + 64 * r;
-            const float4 va = *reinterpret_cast<const float4 *>(T + (a0 + row) * m_pad + k0 + lcol);
-            const float4 vb = *reinterpret_cast<const float4 *>(T + (b0 + row) * m_pad + k0 + lcol);
-            As[buf][lcol + 0][row] = va.x;
-            As[buf][lcol + 1][row] = va.y;
-            As[buf][lcol + 2][row] = va.z;
-            As[buf][lcol + 3][row] = va.w;
-            Bs[buf][lcol + 0][row] = vb.x;
-            Bs[buf][lcol + 1][row] = vb.y;
-            Bs[buf][lcol + 2][row] = vb.z;
-            Bs[buf][lcol + 3][row] = vb.w;
+            const int kk = lk + 8 * r;
+            const float4 va = *reinterpret_cast<const float4 *>(T + (k0 + kk) * d_pad + a0 + lg);
+            const float4 vb = *reinterpret_cast<const float4 *>(T + (k0 + kk) * d_pad + b0 + lg);
+            *reinterpret_cast<float4 *>(&As[buf][kk][lg]) = va;
+            *reinterpret_cast<float4 *>(&Bs[buf][kk][lg]) = vb;
         }
     };
     auto fold = [&]() {
@@ -368,14 +351,14 @@ __global__ void __launch_bounds__(256) k_syrk_f32(const float *__restrict__ T, i
     for (int p = 0; p < 8; ++p) {
         const int64_t a = a0 + (p < 4 ? ty * 4 + p : 64 + ty * 4 + p - 4);
         if (a >= d) continue;
-        const double ba = bias ? bias[a] : 0.0, ca = colsum_c[a];
+        const double ba = shift ? shift[a] : 0.0, ca = colsum_c[a];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const int64_t b = b0 + (q < 4 ? tx * 4 + q : 64 + tx * 4 + q - 4);
             if (b >= d || b < a) continue;
             double v = acc64[(p * 8 + q) * 256 + tid];
-            if (bias) {
-                const double bb = bias[b], cb = colsum_c[b];
+            if (shift) {
+                const double bb = shift[b], cb = colsum_c[b];
                 v = v - ba * cb - ca * bb - nk * ba * bb;
             }
             G[a * d + b] += v;
@@ -395,21 +378,23 @@ int launch_syrk_fold(const GramWork &w, int64_t m, const DevScale &t, double *gr
     if (w.precision == CREST_GRAM_FP64) {
         const int64_t nb = ceil_div(w.d, 64);
         const int64_t tiles = nb * (nb + 1) / 2;
-        prof::Scope ps("syrk_fp64", st);
-        k_syrk_f64<<<(unsigned)tiles, 256, 0, st>>>((const double *)w.tile, w.d, m_pad, nb, gram);
+        {
+            prof::Scope ps("syrk_fp64", st);
+            k_syrk_f64<<<(unsigned)tiles, 256, 0, st>>>((const double *)w.tile, w.d, w.d_pad, m_pad, nb, gram);
+        }
         CREST_CUDA_TRY(cudaGetLastError());
-        k_colsum_f64<<<(unsigned)ceil_div(w.d, 128), 128, 0, st>>>((const double *)w.tile, w.d, m_pad, m, colsum);
+        k_colsum_f64<<<(unsigned)ceil_div(w.d, 128), 128, 0, st>>>((const double *)w.tile, w.d, w.d_pad, m, colsum);
         CREST_CUDA_TRY(cudaGetLastError());
         return CREST_OK;
     }
-    const double *bias = t.scale ? t.bias : nullptr;
+    const double *shift = t.scale ? w.shift : nullptr;  // the tile's exact zero-entry value
     if (w.precision == CREST_GRAM_FP32) {
         const int64_t nb = w.d_pad / kBM;
         const int64_t tiles = nb * (nb + 1) / 2;
         prof::Scope ps("syrk_fp32", st);
         CREST_CUDA_TRY(
             cudaFuncSetAttribute(k_syrk_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSyrkF32Smem));
-        k_syrk_f32<<<(unsigned)tiles, 256, kSyrkF32Smem, st>>>((const float *)w.tile, w.d, m_pad, nb, bias,
+        k_syrk_f32<<<(unsigned)tiles, 256, kSyrkF32Smem, st>>>((const float *)w.tile, w.d, w.d_pad, m_pad, nb, shift,
                                                               w.colsum_chunk, w.n_kept, gram);
         CREST_CUDA_TRY(cudaGetLastError());
     } else {

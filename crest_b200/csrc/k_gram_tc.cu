@@ -1,9 +1,10 @@
 // Product-form Gram (K4): split-BF16 ("bf16x3") SYRK on the sm_100a tcgen05
 // tensor cores.
 //
-// Each tile value z = hi + lo (hi = bf16(z), lo = bf16(z - hi)) is stored as
-// two gene-major bf16 tiles.  One CTA owns one 128x128 upper-triangular block
-// (a-genes x b-genes) of G and contracts the chunk's cells (K):
+// Each tile value z = hi + lo (hi = bf16(z), lo = bf16(z - hi)) is stored in
+// two cell-major bf16 tiles (one row of genes per cell), so both operands are
+// MN-major for the tensor core.  One CTA owns one 128x128 upper-triangular
+// block (a-genes x b-genes) of G and contracts the chunk's cells (K):
 //
 //   G_ab += sum_k hi_a hi_b + hi_a lo_b + lo_a hi_b      (FP32 in TMEM)
 //
@@ -12,17 +13,20 @@
 //              the diagonal) into a 3-deep 128B-swizzled shared-memory ring;
 //   warp 1     allocates all 512 TMEM columns (four 128x128 FP32 accumulators)
 //              and issues the tcgen05.mma instructions from one thread;
-//   warps 2-9  fold each stage's FP32 accumulator into FP64 registers while
-//              the MMAs run into the next accumulator, so FP32 accumulation
-//              never spans more than 64 cells (12 MMAs; the tensor core's
-//              FP32 adder does not round to nearest, so long FP32 chains drift),
-//              and finally add the FP64 block into G with the bias correction
-//              S^T S = Z^T Z - bias c^T - c bias^T - n bias bias^T.
+//   warps 2-9  fold each period's FP32 accumulator (fold stages of 64 cells,
+//              2 by default) into FP64 register sums while the
+//              MMAs run into the next accumulator, so the tensor core's FP32
+//              accumulation never spans more than one period (12 MMAs per
+//              stage; long FP32 chains in the tensor core drift, measured
+//              1.2e-5 relative over 512 cells); at the end the block goes
+//              through shared memory to a coalesced FP64 update of G with the
+//              shift correction S^T S = Z^T Z - shift c^T - c shift^T - n shift shift^T.
 //
 // Every mbarrier wait is bounded (about one second of %globaltimer); on
 // timeout the kernel records an error code, stops issuing work and still
 // releases its TMEM before returning.
 #include <cuda.h>
+#include <stdlib.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
@@ -33,19 +37,23 @@ namespace crest {
 namespace {
 
 constexpr int kTile = 128;         // M = N of one block
-constexpr int kStageCells = 64;    // K per stage: 64 bf16 = 128 B rows (one swizzle atom)
+constexpr int kStageCells = 64;    // K per stage (cells)
+constexpr int kHalf = 64;          // genes per TMA box / MN swizzle atom: 64 bf16 = 128 B
 constexpr int kStages = 3;
 constexpr int kAccBufs = 4;        // TMEM accumulators (4 x 128 columns)
-constexpr int kOperandBytes = kTile * kStageCells * 2;  // 16 KB
+constexpr int kBoxBytes = kHalf * kStageCells * 2;     // 8 KB: 64 genes x 64 cells
+constexpr int kOperandBytes = 2 * kBoxBytes;           // 16 KB: 128 genes x 64 cells
 constexpr int kStageBytes = 4 * kOperandBytes;          // A_hi, A_lo, B_hi, B_lo
-constexpr int kThreads = 320;
+constexpr int kEpiWarps = 8;      // 2 per TMEM lane quadrant, 64 accumulator columns each
+constexpr int kThreads = (2 + kEpiWarps) * 32;
 constexpr uint32_t kTmemCols = 512;
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s
 
 // instruction descriptor, kind::f16: D f32 (bit 4), A bf16 (bits 7-9 = 1),
-// B bf16 (bits 10-12 = 1), both K-major, N>>3 at bit 17, M>>4 at bit 24
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kTile >> 3) << 17) |
-                            ((uint32_t)(kTile >> 4) << 24);
+// B bf16 (bits 10-12 = 1), A and B MN-major (bits 15, 16), N>>3 at bit 17,
+// M>>4 at bit 24
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                            ((uint32_t)(kTile >> 3) << 17) | ((uint32_t)(kTile >> 4) << 24);
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return (uint32_t)__cvta_generic_to_shared(p);
@@ -70,30 +78,36 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// try_wait suspends the thread until the phase completes or the hint (ns)
+// expires, so a waiting role costs no issue slots and wakes on completion.
 __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(20000u)
         : "memory");
     return ok != 0;
 }
 
-// Bounded wait: false (and an error code in *err) after kWaitNs.
+// Bounded wait: false (and an error code in *err) after kWaitNs.  The error
+// word (global memory) is only looked at on the slow path, every 64 polls,
+// so another role's failure also ends this wait.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
     if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = globaltimer();
-    while (!mbar_try(bar, parity)) {
-        if (globaltimer() - t0 > kWaitNs) {
-            atomicCAS(err, 0, code);
-            return false;
+    for (uint32_t n = 1;; ++n) {
+        if (mbar_try(bar, parity)) return true;
+        if ((n & 63u) == 0) {
+            if (globaltimer() - t0 > kWaitNs) {
+                atomicCAS(err, 0, code);
+                return false;
+            }
+            if (*(volatile int *)err) return false;
         }
-        if (*(volatile int *)err) return false;
     }
-    return true;
 }
 
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
@@ -104,9 +118,12 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
-// UMMA shared-memory descriptor: K-major, 128B swizzle, 8-row groups 1024 B apart.
+// UMMA shared-memory descriptor of an MN-major operand with 128B swizzle:
+// 64-element MN atoms (128 B rows, one row per K index), atoms along MN
+// kBoxBytes apart (leading byte offset), groups of 8 K rows 1024 B apart
+// (stride byte offset).
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(kBoxBytes >> 4) << 16) | ((uint64_t)(1024 >> 4) << 32) |
            ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
 
@@ -140,6 +157,17 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void tri_decode(int t, int nb, int &bi, int &bj) {
@@ -155,6 +183,8 @@ __device__ __forceinline__ void tri_decode(int t, int nb, int &bi, int &bj) {
 struct TcArgs {
     int64_t d, d_pad;
     int n_stages;          // K stages in this launch (m_pad / 64)
+    int m_pad;             // cells in the tile (row offset of the lo tile)
+    int fold;              // stages accumulated in FP32 before each FP64 fold
     int nb;                // 128-blocks along d_pad
     const double *bias;    // [d] or nullptr
     const double *colsum;  // [d] colsum of S for this chunk
@@ -167,6 +197,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_bf16x3(const __grid_consta
     extern __shared__ uint8_t smem_dyn[];
     __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages], acc_full[kAccBufs], acc_empty[kAccBufs];
     __shared__ uint32_t tmem_base_sh;
+    __shared__ int epi_ok;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int bi, bj;
@@ -177,13 +208,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_bf16x3(const __grid_consta
     uint8_t *ring = smem_dyn + (((raw + 1023u) & ~1023u) - raw);
 
     if (threadIdx.x == 0) {
+        epi_ok = 1;
         for (int s = 0; s < kStages; ++s) {
             mbar_init(&full_bar[s], 1);
             mbar_init(&empty_bar[s], 1);
         }
         for (int b = 0; b < kAccBufs; ++b) {
             mbar_init(&acc_full[b], 1);
-            mbar_init(&acc_empty[b], 8);
+            mbar_init(&acc_empty[b], kEpiWarps);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -197,105 +229,133 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_bf16x3(const __grid_consta
     tc_fence_after();
     const uint32_t tmem = tmem_base_sh;
 
+    // Waits are made by lane 0 and broadcast, so every role warp stays
+    // converged (the .sync.aligned tcgen05 instructions need the whole warp).
+    auto warp_wait = [&](uint64_t *bar, uint32_t parity, int code) -> bool {
+        int got = 0;
+        if (lane == 0) got = mbar_wait(bar, parity, a.err, code) ? 1 : 0;
+        return __shfl_sync(0xffffffffu, got, 0) != 0;
+    };
+    const int n_periods = (a.n_stages + a.fold - 1) / a.fold;
+
     if (warp == 0) {
         // ---------------------------------------------------------- producer
-        if (lane == 0) {
-            const uint32_t bytes = diag ? 2 * kOperandBytes : 4 * kOperandBytes;
-            const int ya = bi * kTile, yb = bj * kTile, lo_off = (int)a.d_pad;
-            for (int i = 0; i < a.n_stages; ++i) {
-                const int s = i % kStages;
-                if (i >= kStages && !mbar_wait(&empty_bar[s], ((i / kStages) - 1) & 1, a.err, 1)) break;
+        const uint32_t bytes = diag ? 2 * kOperandBytes : 4 * kOperandBytes;
+        const int xa = bi * kTile, xb = bj * kTile, lo_off = a.m_pad;
+        int issued = 0;
+        for (int i = 0; i < a.n_stages; ++i) {
+            const int s = i % kStages;
+            if (i >= kStages && !warp_wait(&empty_bar[s], ((i / kStages) - 1) & 1, 1)) break;
+            if (lane == 0) {
                 uint8_t *st = ring + (size_t)s * kStageBytes;
                 mbar_expect_tx(&full_bar[s], bytes);
-                const int x = i * kStageCells;
-                tma_load_2d(st, &tmap, &full_bar[s], x, ya);
-                tma_load_2d(st + kOperandBytes, &tmap, &full_bar[s], x, lo_off + ya);
+                const int y = i * kStageCells;  // first cell of the stage
+                // operand = two 64-gene boxes side by side (MN atoms kBoxBytes apart)
+                tma_load_2d(st, &tmap, &full_bar[s], xa, y);
+                tma_load_2d(st + kBoxBytes, &tmap, &full_bar[s], xa + kHalf, y);
+                tma_load_2d(st + kOperandBytes, &tmap, &full_bar[s], xa, lo_off + y);
+                tma_load_2d(st + kOperandBytes + kBoxBytes, &tmap, &full_bar[s], xa + kHalf, lo_off + y);
                 if (!diag) {
-                    tma_load_2d(st + 2 * kOperandBytes, &tmap, &full_bar[s], x, yb);
-                    tma_load_2d(st + 3 * kOperandBytes, &tmap, &full_bar[s], x, lo_off + yb);
+                    tma_load_2d(st + 2 * kOperandBytes, &tmap, &full_bar[s], xb, y);
+                    tma_load_2d(st + 2 * kOperandBytes + kBoxBytes, &tmap, &full_bar[s], xb + kHalf, y);
+                    tma_load_2d(st + 3 * kOperandBytes, &tmap, &full_bar[s], xb, lo_off + y);
+                    tma_load_2d(st + 3 * kOperandBytes + kBoxBytes, &tmap, &full_bar[s], xb + kHalf, lo_off + y);
                 }
             }
-            // drain: every stage release (tcgen05.commit arrival) lands before the CTA exits
-            for (int i = max(0, a.n_stages - kStages); i < a.n_stages; ++i)
-                if (!mbar_wait(&empty_bar[i % kStages], (i / kStages) & 1, a.err, 5)) break;
+            __syncwarp();
+            issued = i + 1;
         }
+        // drain: every stage release (tcgen05.commit arrival) lands before the CTA exits
+        for (int i = max(0, issued - kStages); i < issued; ++i)
+            if (!warp_wait(&empty_bar[i % kStages], (i / kStages) & 1, 5)) break;
     } else if (warp == 1) {
         // --------------------------------------------------------- MMA issuer
-        if (lane == 0) {
-            for (int i = 0; i < a.n_stages; ++i) {
-                const int buf = i % kAccBufs;
-                if (i >= kAccBufs && !mbar_wait(&acc_empty[buf], ((i / kAccBufs) - 1) & 1, a.err, 2)) break;
-                const uint32_t d_tmem = tmem + (uint32_t)(buf * kTile);
-                {
-                    const int s = i % kStages;
-                    if (!mbar_wait(&full_bar[s], (i / kStages) & 1, a.err, 3)) break;
-                    tc_fence_after();
+        bool ok = true;
+        for (int p = 0; p < n_periods && ok; ++p) {
+            const int buf = p % kAccBufs;
+            if (p >= kAccBufs && !warp_wait(&acc_empty[buf], ((p / kAccBufs) - 1) & 1, 2)) break;
+            const uint32_t d_tmem = tmem + (uint32_t)(buf * kTile);
+            const int i0 = p * a.fold, i1 = min(a.n_stages, i0 + a.fold);
+            for (int i = i0; i < i1; ++i) {
+                const int s = i % kStages;
+                if (!warp_wait(&full_bar[s], (i / kStages) & 1, 3)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                if (lane == 0) {
                     const uint32_t st = smem_u32(ring + (size_t)s * kStageBytes);
                     const uint32_t a_hi = st, a_lo = st + kOperandBytes;
                     const uint32_t b_hi = diag ? a_hi : st + 2 * kOperandBytes;
                     const uint32_t b_lo = diag ? a_lo : st + 3 * kOperandBytes;
 #pragma unroll
                     for (int kk = 0; kk < kStageCells / 16; ++kk) {
-                        const uint32_t off = kk * 32;  // 16 bf16 along K inside the 128-B row
-                        const uint32_t first = kk == 0 ? 0u : 1u;
+                        const uint32_t off = kk * 16 * 128;  // 16 K rows of 128 B = two 8-row groups
+                        const uint32_t first = (i == i0 && kk == 0) ? 0u : 1u;
                         umma_bf16(d_tmem, umma_desc(a_hi + off), umma_desc(b_hi + off), first);
                         umma_bf16(d_tmem, umma_desc(a_hi + off), umma_desc(b_lo + off), 1u);
                         umma_bf16(d_tmem, umma_desc(a_lo + off), umma_desc(b_hi + off), 1u);
                     }
                     umma_commit(&empty_bar[s]);  // stage reusable once these MMAs complete
                 }
-                umma_commit(&acc_full[buf]);
+                __syncwarp();
             }
+            if (ok && lane == 0) umma_commit(&acc_full[buf]);
+            __syncwarp();
         }
     } else {
         // ----------------------------------------------------------- epilogue
         const int q = warp & 3;              // TMEM lane quadrant this warp may access
-        const int h = (warp - 2) >> 2;       // column half: 0 -> 0..63, 1 -> 64..127
+        const int h = (warp - 2) >> 2;       // column group: 64 h .. 64 h + 63
         const int row = q * 32 + lane;
-        double acc[64];
+        double acc[64];                      // FP64 sums of the periods
 #pragma unroll
         for (int j = 0; j < 64; ++j) acc[j] = 0.0;
         bool ok = true;
-        for (int p = 0; p < a.n_stages; ++p) {
+        for (int p = 0; p < n_periods; ++p) {
             const int buf = p % kAccBufs;
-            // one lane waits, the warp reconverges before the .sync.aligned TMEM loads
-            int got = 0;
-            if (lane == 0) got = mbar_wait(&acc_full[buf], (p / kAccBufs) & 1, a.err, 4) ? 1 : 0;
-            got = __shfl_sync(0xffffffffu, got, 0);
-            if (!got) {
+            if (!warp_wait(&acc_full[buf], (p / kAccBufs) & 1, 4)) {
                 ok = false;
                 break;
             }
             tc_fence_after();
             const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * kTile + h * 64);
-            float v[32];
-            tmem_ld32(taddr, v);
-            tmem_wait_ld();
 #pragma unroll
-            for (int j = 0; j < 32; ++j) acc[j] += (double)v[j];
-            tmem_ld32(taddr + 32, v);
-            tmem_wait_ld();
+            for (int g = 0; g < 4; ++g) {  // 16 columns at a time keeps the register footprint down
+                float v[16];
+                tmem_ld16(taddr + 16 * g, v);
+                tmem_wait_ld();
 #pragma unroll
-            for (int j = 0; j < 32; ++j) acc[32 + j] += (double)v[j];
+                for (int j = 0; j < 16; ++j) acc[16 * g + j] += (double)v[j];
+            }
             tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&acc_empty[buf]);
+            if (lane == 0) mbar_arrive(&acc_empty[buf]);  // accumulator read out
         }
+        // Stage the FP64 block in the operand ring (idle once the last
+        // accumulator has been seen: every MMA has read its operands), then
+        // update G row by row with coalesced accesses.
+        double *stage = reinterpret_cast<double *>(ring);
+        constexpr int kPitch = kTile + 1;
+        if (!ok) atomicExch(&epi_ok, 0);
         if (ok) {
-            const int64_t ga = (int64_t)bi * kTile + row;
-            if (ga < a.d) {
-                const double nk = (double)*a.n_kept;
+#pragma unroll
+            for (int j = 0; j < 64; ++j) stage[row * kPitch + h * 64 + j] = acc[j];
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(kEpiWarps * 32) : "memory");  // the epilogue warps
+        if (epi_ok) {
+            const int e = warp - 2;
+            const double nk = (double)*a.n_kept;
+            for (int r = e; r < kTile; r += kEpiWarps) {
+                const int64_t ga = (int64_t)bi * kTile + r;
+                if (ga >= a.d) break;
                 const double ba = a.bias ? a.bias[ga] : 0.0, ca = a.colsum[ga];
                 double *grow = a.G + ga * a.d;
-#pragma unroll
-                for (int j = 0; j < 64; ++j) {
-                    const int64_t gb = (int64_t)bj * kTile + h * 64 + j;
+                for (int cc = lane; cc < kTile; cc += 32) {
+                    const int64_t gb = (int64_t)bj * kTile + cc;
                     if (gb >= a.d || gb < ga) continue;
-                    double v = acc[j];
-                    if (a.bias) {
-                        const double bb = a.bias[gb], cb = a.colsum[gb];
-                        v = v - ba * cb - ca * bb - nk * ba * bb;
-                    }
+                    double v = stage[r * kPitch + cc];
+                    if (a.bias) v = v - ba * a.colsum[gb] - ca * a.bias[gb] - nk * ba * a.bias[gb];
                     grow[gb] += v;
                 }
             }
@@ -331,6 +391,15 @@ struct ErrFlag {
 static ErrFlag g_tc_err[64];
 
 // Device error word of the current device (0 = no bounded wait has timed out).
+// FP32 accumulation period in 64-cell stages (CREST_TC_FOLD, default 2: 128
+// cells; at 1M cells 1, 2 and 4 stages all keep the top-50 subspace within
+// 0.007 degree of the FP64 Gram, 8 stages drift past 0.01 degree).
+int tc_fold_stages() {
+    const char *e = getenv("CREST_TC_FOLD");
+    int v = e ? atoi(e) : 2;
+    return v < 1 ? 1 : (v > 64 ? 64 : v);
+}
+
 int *tc_error_word() {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -361,11 +430,11 @@ int syrk_bf16x3_fold(const GramWork &w, int64_t m_pad, const DevScale &t, double
     CREST_REQUIRE(enc != nullptr, CREST_ECUDA, "cuTensorMapEncodeTiled is unavailable");
     int *err = tc_error_word();
     CREST_REQUIRE(err != nullptr, CREST_ENOMEM, "could not allocate the pipeline error word");
-    // hi rows [0, d_pad) then lo rows [d_pad, 2 d_pad), cells contiguous
+    // cell rows of d_pad genes: hi rows [0, m_pad) then lo rows [m_pad, 2 m_pad)
     CUtensorMap map;
-    cuuint64_t dims[2] = {(cuuint64_t)m_pad, (cuuint64_t)(2 * w.d_pad)};
-    cuuint64_t strides[1] = {(cuuint64_t)m_pad * 2};
-    cuuint32_t box[2] = {kStageCells, kTile};
+    cuuint64_t dims[2] = {(cuuint64_t)w.d_pad, (cuuint64_t)(2 * m_pad)};
+    cuuint64_t strides[1] = {(cuuint64_t)w.d_pad * 2};
+    cuuint32_t box[2] = {kHalf, kStageCells};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, w.tile, dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -375,8 +444,10 @@ int syrk_bf16x3_fold(const GramWork &w, int64_t m_pad, const DevScale &t, double
     a.d = w.d;
     a.d_pad = w.d_pad;
     a.n_stages = (int)(m_pad / kStageCells);
+    a.m_pad = (int)m_pad;
     a.nb = (int)(w.d_pad / kTile);
-    a.bias = t.scale ? t.bias : nullptr;
+    a.fold = tc_fold_stages();
+    a.bias = t.scale ? w.shift : nullptr;  // bf16-rounded bias: the exact tile value of zeros
     a.colsum = w.colsum_chunk;
     a.n_kept = w.n_kept;
     a.G = gram;

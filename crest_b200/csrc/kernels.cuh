@@ -42,6 +42,8 @@ struct GramWork {
     double *colsum_chunk;   // [d] FP64 column sums of S for the current tile
     int64_t *n_kept;        // [1] kept cells in the current tile
     float *part32;          // [d_pad * d_pad] FP32 partial (FP32 / BF16X3)
+    double *shift;          // [d_pad] tile value of a zero entry: bias rounded to the tile's
+                            // precision, so the (repeated) zeros are stored exactly
 };
 
 size_t gram_tile_bytes(int precision, int64_t d_pad, int64_t m_cap);

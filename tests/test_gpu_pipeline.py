@@ -53,12 +53,32 @@ def max_angle(A, B):
     return float(op.principal_angles_deg(A, B).max())
 
 
-def aligned_rel_err(X, R):
+def aligned_rel_err(X, R, cols=None):
+    """Largest per-component relative score error after sign alignment."""
     X = X.astype(np.float64)
     R = R.astype(np.float64)
     s = np.sign((X * R).sum(0))
     s[s == 0] = 1
-    return float(np.max(np.linalg.norm(X * s - R, axis=0) / np.linalg.norm(R, axis=0)))
+    err = np.linalg.norm(X * s - R, axis=0) / np.linalg.norm(R, axis=0)
+    return float(np.max(err if cols is None else err[cols]))
+
+
+def procrustes_rel_err(X, R):
+    """Relative score error after the best orthogonal alignment: scores of a
+    near-degenerate pair of components are only defined up to a rotation."""
+    X = X.astype(np.float64)
+    R = R.astype(np.float64)
+    U, _, Vt = np.linalg.svd(X.T @ R)
+    return float(np.linalg.norm(X @ (U @ Vt) - R) / np.linalg.norm(R))
+
+
+def separated(variance, rel_gap=2e-3):
+    """Components whose eigenvalue is at least rel_gap away (relatively) from both neighbours."""
+    v = np.asarray(variance, np.float64)
+    gaps = np.full(len(v), np.inf)
+    gaps[:-1] = np.minimum(gaps[:-1], (v[:-1] - v[1:]) / v[:-1])
+    gaps[1:] = np.minimum(gaps[1:], (v[:-1] - v[1:]) / v[:-1])
+    return np.flatnonzero(gaps[:-1] >= rel_gap) if len(v) > 1 else np.arange(len(v))
 
 
 @pytest.mark.parametrize("name", ["small", "pbmc3k_like"])
@@ -86,7 +106,13 @@ def test_pipeline_matches_reference_golden(name, precision):
     X = bf.obsm["X_pca"]
     R = g["X_pca"]
     assert max_angle(X[: len(R)], R) <= 0.01
-    assert aligned_rel_err(X[: len(R)], R) <= 1e-4
+    if precision == "fp64":
+        assert aligned_rel_err(X[: len(R)], R) <= 1e-4
+    else:
+        # reduced-precision Gram: every component with a real eigengap matches
+        # to 1e-4; the near-degenerate tail is checked as a subspace
+        assert aligned_rel_err(X[: len(R)], R, separated(g["variance"])) <= 1e-4
+        assert procrustes_rel_err(X[: len(R)], R) <= 1e-4
 
 
 def test_chunking_store_and_residency_invariance():
@@ -113,4 +139,6 @@ def test_precision_forms_against_fp64():
         L0 = ref.uns["pca"]["projection"]["loadings"]
         L1 = got.uns["pca"]["projection"]["loadings"]
         assert float(op.subspace_angles_deg(L0, L1).max()) <= 0.01
-        assert aligned_rel_err(got.obsm["X_pca"], ref.obsm["X_pca"]) <= 1e-4
+        sep = separated(ref.uns["pca"]["variance"])
+        assert aligned_rel_err(got.obsm["X_pca"], ref.obsm["X_pca"], sep) <= 1e-4
+        assert procrustes_rel_err(got.obsm["X_pca"], ref.obsm["X_pca"]) <= 1e-4
