@@ -86,7 +86,7 @@ struct Ctx {
     std::mutex mu;
     bool ready = false;
     cudaStream_t st = nullptr;
-    DevBuf genes, values, span_ptr, span_cell, cell_map, gene_map, flag, sub_map;
+    DevBuf genes, values, span_ptr, span_cell, cell_map, gene_map, flag, sub_map, code;
     DevBuf out0, out1, out2, out3, out4, out5;
     DevBuf mean, std_, bias, gram, colsum, vecs, vals, total, loadings;
     GramBufs gb;
@@ -227,12 +227,18 @@ static int check_sub_map(const int32_t *sub_map, int64_t n_vars, int64_t d) {
     return CREST_OK;
 }
 
-int gram_over_chunk(const DevChunk &dc, const int32_t *sub_map, const DevScale &ds, GramWork &w,
+int stage_hvg_code(const DevChunk &dc, const int32_t *sub_map, int64_t n_vars, int64_t d, DevBuf &buf,
+                   cudaStream_t st) {
+    CREST_TRY(buf.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(dc.n_gene_map, 1)));
+    return launch_hvg_code(dc, sub_map, n_vars, d, buf.as<int32_t>(), st);
+}
+
+int gram_over_chunk(const DevChunk &dc, const int32_t *code, const DevScale &ds, GramWork &w,
                            double *gram, double *colsum, cudaStream_t st) {
     for (int64_t s0 = 0; s0 < dc.n_spans; s0 += w.m_cap) {
         const int64_t n = std::min(w.m_cap, dc.n_spans - s0);
         const DevChunk sc = slice(dc, s0, n);
-        CREST_TRY(launch_densify(sc, sub_map, ds, w, st));
+        CREST_TRY(launch_densify(sc, code, ds, w, st));
         CREST_TRY(launch_syrk_fold(w, n, ds, gram, colsum, st));
     }
     return CREST_OK;
@@ -362,7 +368,8 @@ int crest_gram_accumulate(const crest_chunk *chunk, const int32_t *sub_map, int6
     GramWork w;
     const int64_t m_cap = std::min<int64_t>(tile_cells_default(), round_up(std::max<int64_t>(s.n, 1), 64));
     CREST_TRY(x->gb.ensure(w, d, precision, m_cap));
-    CREST_TRY(gram_over_chunk(dc, x->sub_map.as<int32_t>(), ds, w, x->gram.as<double>(), x->colsum.as<double>(), st));
+    CREST_TRY(stage_hvg_code(dc, x->sub_map.as<int32_t>(), n_vars, d, x->code, st));
+    CREST_TRY(gram_over_chunk(dc, x->code.as<int32_t>(), ds, w, x->gram.as<double>(), x->colsum.as<double>(), st));
     if (precision == CREST_GRAM_BF16X3) {
         CREST_CUDA_TRY(cudaStreamSynchronize(st));
         CREST_TRY(tc_check_error());
@@ -444,8 +451,9 @@ int crest_project(const crest_chunk *chunk, const int32_t *sub_map, int64_t n_va
     CREST_TRY(stage_scale(x->mean, x->std_, x->bias, scale, d, ds, st));
     CREST_TRY(upload(x->loadings, loadings, d * k, st));
     CREST_TRY(zeros<float>(x->out3, s.n * k, st));
-    CREST_TRY(launch_project(dc, x->sub_map.as<int32_t>(), ds, x->loadings.as<double>(), (int)k, x->out3.as<float>(),
-                             1, st));
+    CREST_TRY(stage_hvg_code(dc, x->sub_map.as<int32_t>(), n_vars, d, x->code, st));
+    CREST_TRY(launch_project(dc, x->code.as<int32_t>(), d, ds, x->loadings.as<double>(), (int)k,
+                             x->out3.as<float>(), 1, st));
     std::vector<float> part(s.n * k);
     if (s.n * k)
         CREST_CUDA_TRY(cudaMemcpyAsync(part.data(), x->out3.ptr, 4 * s.n * k, cudaMemcpyDeviceToHost, st));

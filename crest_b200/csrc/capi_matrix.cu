@@ -27,7 +27,7 @@ struct crest_matrix {
     crest::DevBuf buf_idx[2], buf_val[2];
     cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
     // per-pass staging
-    crest::DevBuf cell_map, gene_map, flag, sub_map, mean, std_, bias;
+    crest::DevBuf cell_map, gene_map, flag, sub_map, code, mean, std_, bias;
     crest::DevBuf out[5];
 };
 
@@ -373,8 +373,9 @@ int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
     DevScale ds;
     CREST_TRY(stage_scale(m->mean, m->std_, m->bias, scale, p->d, ds, st));
     const DevChunk proto = base_chunk(m, target_sum, log1p);
+    CREST_TRY(stage_hvg_code(proto, m->sub_map.as<int32_t>(), n_vars, p->d, m->code, st));
     CREST_TRY(for_each_piece(m, proto, p->w.m_cap, [&](const DevChunk &c) {
-        return gram_over_chunk(c, m->sub_map.as<int32_t>(), ds, p->w, p->gram.as<double>(), p->colsum.as<double>(), st);
+        return gram_over_chunk(c, m->code.as<int32_t>(), ds, p->w, p->gram.as<double>(), p->colsum.as<double>(), st);
     }));
     p->stats.gram_ms = t.stop();
     CREST_CUDA_TRY(cudaGetLastError());
@@ -459,8 +460,9 @@ int crest_pca_project(crest_pca *p, crest_matrix *m, const int64_t *cell_map, co
         k_fill_scores<<<(unsigned)ceil_div(n_rows * p->k, 256), 256, 0, st>>>(p->shift.as<double>(), n_rows, p->k, X);
     CREST_CUDA_TRY(cudaGetLastError());
     const DevChunk proto = base_chunk(m, target_sum, log1p);
+    CREST_TRY(stage_hvg_code(proto, m->sub_map.as<int32_t>(), n_vars, p->d, m->code, st));
     CREST_TRY(for_each_piece(m, proto, m->n_cells, [&](const DevChunk &c) {
-        return launch_project(c, m->sub_map.as<int32_t>(), ds, p->vecs.as<double>(), (int)p->k, X, 0, st);
+        return launch_project(c, m->code.as<int32_t>(), p->d, ds, p->vecs.as<double>(), (int)p->k, X, 0, st);
     }));
     if (out_mem != CREST_MEM_DEVICE && n_rows * p->k)
         CREST_CUDA_TRY(cudaMemcpyAsync(out, X, 4 * (size_t)(n_rows * p->k), cudaMemcpyDeviceToHost, st));

@@ -63,8 +63,8 @@ struct HostBuf {
     template <class T> T *as() const { return reinterpret_cast<T *>(ptr); }
 };
 
-inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
-inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
+__host__ __device__ inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+__host__ __device__ inline int64_t round_up(int64_t a, int64_t b) { return ceil_div(a, b) * b; }
 
 // Device view of one chunk of the raw count matrix (the reference's
 // ChunkView, src/kernels.rs:24-32).  Entry e of span i lies in

@@ -72,8 +72,12 @@ inline DevChunk slice(const DevChunk &c, int64_t s0, int64_t n) {
     return r;
 }
 
-int gram_over_chunk(const DevChunk &dc, const int32_t *sub_map, const DevScale &ds, GramWork &w, double *gram,
+// code: per-gene HVG codes from launch_hvg_code
+int gram_over_chunk(const DevChunk &dc, const int32_t *code, const DevScale &ds, GramWork &w, double *gram,
                     double *colsum, cudaStream_t st);
+// Per-gene HVG codes of a chunk's gene_map and sub_map into buf.
+int stage_hvg_code(const DevChunk &dc, const int32_t *sub_map, int64_t n_vars, int64_t d, DevBuf &buf,
+                   cudaStream_t st);
 
 // Upload mean/std of d genes and derive bias = clip(-mean/std).
 int stage_scale(DevBuf &mean, DevBuf &std_, DevBuf &bias, const crest_scale *t, int64_t d, DevScale &ds,

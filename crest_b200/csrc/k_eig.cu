@@ -7,12 +7,23 @@
 //
 // d <= 160: cyclic Jacobi on the whole matrix in one CTA (matrix in shared
 // memory, round-robin parallel ordering).
-// d > 160: Chebyshev-filtered subspace iteration (Zhou & Saad, 2007) on a
-// block of p = k + 32 (rounded to 16) vectors: Rayleigh-Ritz with the same
-// Jacobi kernel on the p x p projected matrix, a degree-m Chebyshev filter
-// that damps the spectrum below the smallest Ritz value, and classical
-// Gram-Schmidt with re-orthogonalisation.  Stops when every wanted residual
-// ||C v - theta v|| is below tol * theta_1.
+//
+// d > 160: Chebyshev-filtered subspace iteration (Zhou & Saad 2007) with
+// locking, on a block of p = k + 32 (rounded to 16) vectors:
+//  * a short Lanczos run (full re-orthogonalisation) brackets the spectrum;
+//    the filter damps [lambda_min, a] with a = the smallest active Ritz
+//    value, so eigenvalues far from zero (scaled single-cell data: a dense
+//    bulk near 1) still separate quickly;
+//  * converged leading Ritz pairs are locked; the filter then acts on the
+//    remaining columns only, keeping the dynamic range among active columns
+//    small (one dominant component no longer swamps the bulk edge);
+//  * the filter degree follows the estimated gap: enough growth per outer
+//    step for the weakest wanted value, bounded so the block stays well
+//    conditioned for Cholesky QR;
+//  * orthonormalisation is shifted Cholesky QR (Fukaya et al. 2020) built
+//    from split-K FP64 GEMMs, Rayleigh-Ritz uses the same Jacobi kernel on
+//    the p x p projected matrix.
+// Stops when every wanted residual ||C v - theta v|| <= tol * theta_1.
 #include <math.h>
 
 #include <algorithm>
@@ -25,6 +36,8 @@ namespace crest {
 namespace {
 
 constexpr int kJacobiMax = 160;
+constexpr int kJacobiSmemV = 112;  // V also kept in shared memory up to this size
+constexpr int kLanczos = 48;
 
 // ------------------------------------------------------------ centring
 __global__ void k_centre(const double *__restrict__ G, const double *__restrict__ c, int64_t d, double n,
@@ -44,31 +57,9 @@ __global__ void k_trace(const double *__restrict__ C, int64_t d, double *total) 
     *total = s;
 }
 
-// Gershgorin upper bound of the spectrum: max_i sum_j |C[i][j]|
-__global__ void k_row_abs_max(const double *__restrict__ C, int64_t d, double *out) {
-    __shared__ double red[32];
-    double best = 0.0;
-    for (int64_t i = blockIdx.x; i < d; i += gridDim.x) {
-        double s = 0.0;
-        for (int64_t j = threadIdx.x; j < d; j += blockDim.x) s += fabs(C[i * d + j]);
-        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-            for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (threadIdx.x == 0) best = fmax(best, v);
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        unsigned long long *p = reinterpret_cast<unsigned long long *>(out);
-        atomicMax(p, (unsigned long long)__double_as_longlong(best));  // non-negative doubles order as integers
-    }
-}
-
 // ------------------------------------------------------------------ GEMM
-// Column-major FP64 GEMM: O = alpha * op(A) B + beta * X + gamma * Y.
+// Column-major FP64 GEMM: O = alpha * op(A) B + beta * X + gamma * Y, with an
+// optional split of K over gridDim.z (partials to ws, then k_gemm_reduce).
 struct Gemm {
     int M, N, K;
     const double *A;
@@ -83,15 +74,17 @@ struct Gemm {
     double beta;
     const double *Y;
     double gamma;
+    int tB = 0;  // 1: B is given transposed (element (k, n) at B[n + k ldb])
 };
 
-__global__ void __launch_bounds__(256) k_gemm(Gemm g) {
+__global__ void __launch_bounds__(256) k_gemm(Gemm g, int kchunk, double *ws) {
     __shared__ double As[16][64 + 1];
     __shared__ double Bs[16][64 + 1];
     const int m0 = blockIdx.x * 64, n0 = blockIdx.y * 64;
+    const int kb = blockIdx.z * kchunk, ke = min(g.K, kb + kchunk);
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
     double acc[4][4] = {};
-    for (int k0 = 0; k0 < g.K; k0 += 16) {
+    for (int k0 = kb; k0 < ke; k0 += 16) {
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             const int idx = tid + 256 * r;
@@ -105,11 +98,13 @@ __global__ void __launch_bounds__(256) k_gemm(Gemm g) {
             }
             const int m = m0 + mm, k = k0 + kk;
             double v = 0.0;
-            if (m < g.M && k < g.K) v = g.tA ? g.A[k + (int64_t)m * g.lda] : g.A[m + (int64_t)k * g.lda];
+            if (m < g.M && k < ke) v = g.tA ? g.A[k + (int64_t)m * g.lda] : g.A[m + (int64_t)k * g.lda];
             As[kk][mm] = v;
-            const int kb = idx & 15, nn = idx >> 4;
-            const int n = n0 + nn, kB = k0 + kb;
-            Bs[kb][nn] = (n < g.N && kB < g.K) ? g.B[kB + (int64_t)n * g.ldb] : 0.0;
+            const int kq = g.tB ? idx >> 6 : idx & 15, nn = g.tB ? idx & 63 : idx >> 4;
+            const int n = n0 + nn, kB = k0 + kq;
+            double bv = 0.0;
+            if (n < g.N && kB < ke) bv = g.tB ? g.B[n + (int64_t)kB * g.ldb] : g.B[kB + (int64_t)n * g.ldb];
+            Bs[kq][nn] = bv;
         }
         __syncthreads();
 #pragma unroll
@@ -132,6 +127,10 @@ __global__ void __launch_bounds__(256) k_gemm(Gemm g) {
         for (int q = 0; q < 4; ++q) {
             const int m = m0 + tx + 16 * p, n = n0 + ty + 16 * q;
             if (m >= g.M || n >= g.N) continue;
+            if (ws) {
+                ws[((int64_t)blockIdx.z * g.N + n) * g.M + m] = acc[p][q];
+                continue;
+            }
             const int64_t o = m + (int64_t)n * g.ldo;
             double v = g.alpha * acc[p][q];
             if (g.X) v += g.beta * g.X[o];
@@ -140,10 +139,42 @@ __global__ void __launch_bounds__(256) k_gemm(Gemm g) {
         }
 }
 
-int gemm(const Gemm &g, cudaStream_t st) {
+__global__ void k_gemm_reduce(Gemm g, int ksplit, const double *__restrict__ ws) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)g.M * g.N) return;
+    const int m = (int)(idx % g.M), n = (int)(idx / g.M);
+    double s = 0.0;
+    for (int z = 0; z < ksplit; ++z) s += ws[((int64_t)z * g.N + n) * g.M + m];
+    const int64_t o = m + (int64_t)n * g.ldo;
+    double v = g.alpha * s;
+    if (g.X) v += g.beta * g.X[o];
+    if (g.Y) v += g.gamma * g.Y[o];
+    g.O[o] = v;
+}
+
+struct GemmWs {
+    DevBuf ws;
+};
+
+int gemm(const Gemm &g, GemmWs &w, cudaStream_t st) {
     prof::Scope ps("eig_gemm_fp64", st);
-    dim3 grid((unsigned)ceil_div(g.M, 64), (unsigned)ceil_div(g.N, 64));
-    k_gemm<<<grid, 256, 0, st>>>(g);
+    const int mt = (int)ceil_div(g.M, 64), nt = (int)ceil_div(g.N, 64);
+    int ksplit = 1;
+    if (g.K > 0) {
+        const int want = (int)ceil_div(2 * device_sms(), mt * nt);
+        ksplit = std::max(1, std::min(want, (int)ceil_div(g.K, 64)));
+    }
+    if (ksplit == 1) {
+        k_gemm<<<dim3(mt, nt, 1), 256, 0, st>>>(g, std::max(g.K, 1), nullptr);
+        CREST_CUDA_TRY(cudaGetLastError());
+        return CREST_OK;
+    }
+    const int kchunk = (int)round_up(ceil_div(g.K, ksplit), 16);
+    ksplit = (int)ceil_div(g.K, kchunk);
+    CREST_TRY(w.ws.ensure(sizeof(double) * (size_t)ksplit * g.M * g.N));
+    k_gemm<<<dim3(mt, nt, ksplit), 256, 0, st>>>(g, kchunk, w.ws.as<double>());
+    CREST_CUDA_TRY(cudaGetLastError());
+    k_gemm_reduce<<<(unsigned)ceil_div((int64_t)g.M * g.N, 256), 256, 0, st>>>(g, ksplit, w.ws.as<double>());
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
 }
@@ -151,71 +182,68 @@ int gemm(const Gemm &g, cudaStream_t st) {
 // ---------------------------------------------------------------- Jacobi
 // Cyclic Jacobi on a symmetric n_in x n_in column-major matrix (padded to an
 // even n with a decoupled zero row/column).  Round-robin ordering: n/2
-// disjoint pairs per round, n-1 rounds per sweep; each round applies the
-// row rotations, then the column rotations (Rutishauser's formulas, the
-// rotation P with P_pp = P_qq = c, P_pq = s, P_qp = -s zeroes A'_pq in
-// P^T A P).  On exit: vals[i] = A_ii, V (n x n, col-major, global) the
-// accumulated rotations.
-__global__ void __launch_bounds__(1024) k_jacobi(const double *__restrict__ Ain, int n_in, int n, double *V,
-                                                 double *vals, int max_sweeps, int *sweeps_out) {
+// disjoint pairs per round, n-1 rounds per sweep.  The rotation of pair
+// (p, q) is P with P_pp = P_qq = c, P_pq = s, P_qp = -s (Rutishauser's
+// formulas), chosen so that (P^T A P)_pq = 0.  The pairs of a round
+// partition the indices, so A' = J^T A J splits into independent 2x2 blocks
+// (rows of pair i, columns of pair j): each thread updates whole blocks,
+// R_i^T M R_j, and one round costs two barriers.  A rotation is skipped when
+// |A_pq| <= eps sqrt(|A_pp A_qq|) (or below 1e-18 ||A||_F); the solver stops
+// after a sweep without rotations.  The rotations accumulate in V (shared
+// memory when n <= 112, else the n x n global scratch Vwork).  The padding
+// row/column never couples, so the leading n_in x n_in block of V holds the
+// eigenvectors.  On exit: vals[i] = A_ii, Vout (n_in x n_in, col-major).
+template <bool V_SMEM>
+__global__ void __launch_bounds__(1024) k_jacobi(const double *__restrict__ Ain, int n_in, int n, double *Vwork,
+                                                 double *Vout, double *vals, int max_sweeps, int *sweeps_out) {
     extern __shared__ double S[];
     const int ld = n + 1;
+    double *V = V_SMEM ? S + (size_t)n * ld : Vwork;
     __shared__ double cs_[kJacobiMax / 2], sn_[kJacobiMax / 2];
     __shared__ int pp_[kJacobiMax / 2], qq_[kJacobiMax / 2];
-    __shared__ double red[64];
-    __shared__ int done;
+    __shared__ double red[32];
+    __shared__ int rotated;
+    __shared__ double floor_abs;
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int w = tid; w < n * n; w += nt) {
         const int r = w % n, c = w / n;
         S[r + c * ld] = (r < n_in && c < n_in) ? Ain[r + (int64_t)c * n_in] : 0.0;
         V[r + (int64_t)c * n] = (r == c) ? 1.0 : 0.0;
     }
+    // ||A||_F (invariant under the rotations) for the absolute skip floor
+    double ss = 0.0;
+    for (int w = tid; w < n * n; w += nt) {
+        const double v = S[(w % n) + (w / n) * ld];
+        ss += v * v;
+    }
+    for (int o = 16; o; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    if ((tid & 31) == 0) red[tid >> 5] = ss;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int i = 0; i < (nt >> 5); ++i) t += red[i];
+        floor_abs = 1e-18 * sqrt(t);
+        rotated = 0;
+    }
     __syncthreads();
     const int half = n / 2;
+    const double eps = 0x1.0p-52;
     int sweep = 0;
     for (; sweep < max_sweeps; ++sweep) {
-        // convergence: off-diagonal mass relative to the whole matrix
-        double off = 0.0, tot = 0.0;
-        for (int w = tid; w < n * n; w += nt) {
-            const int r = w % n, c = w / n;
-            const double v = S[r + c * ld];
-            tot += v * v;
-            if (r != c) off += v * v;
-        }
-        for (int o = 16; o; o >>= 1) {
-            off += __shfl_xor_sync(0xffffffffu, off, o);
-            tot += __shfl_xor_sync(0xffffffffu, tot, o);
-        }
-        if ((tid & 31) == 0) {
-            red[tid >> 5] = off;
-            red[32 + (tid >> 5)] = tot;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            double so = 0.0, sa = 0.0;
-            for (int i = 0; i < (nt >> 5); ++i) {
-                so += red[i];
-                sa += red[32 + i];
-            }
-            done = (so <= 1e-30 * sa) || so == 0.0;
-        }
-        __syncthreads();
-        if (done) break;
         for (int r = 0; r < n - 1; ++r) {
             if (tid < half) {
-                // positions: 0 fixed, others rotate around the circle
                 const int i = tid;
                 const int a = (i == 0) ? 0 : ((i - 1 + r) % (n - 1)) + 1;
-                const int b = ((n - 1 - i - 1 + r) % (n - 1)) + 1;
+                const int b = ((n - 2 - i + r) % (n - 1)) + 1;
                 const int p = a < b ? a : b, q = a < b ? b : a;
-                const double apq = S[p + q * ld];
+                const double apq = S[p + q * ld], app = S[p + p * ld], aqq = S[q + q * ld];
                 double c = 1.0, s = 0.0;
-                if (apq != 0.0) {
-                    const double app = S[p + p * ld], aqq = S[q + q * ld];
+                if (fabs(apq) > fmax(eps * sqrt(fabs(app * aqq)), floor_abs)) {
                     const double tau = (aqq - app) / (2.0 * apq);
                     const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
                     c = 1.0 / sqrt(1.0 + t * t);
                     s = t * c;
+                    rotated = 1;
                 }
                 cs_[i] = c;
                 sn_[i] = s;
@@ -223,44 +251,69 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double *__restrict__ Ain,
                 qq_[i] = q;
             }
             __syncthreads();
-            // rows p, q  <- P^T A
-            for (int w = tid; w < half * n; w += nt) {
-                const int i = w % half, j = w / half;
-                const int p = pp_[i], q = qq_[i];
-                const double c = cs_[i], s = sn_[i];
-                if (s == 0.0) continue;
-                const double x = S[p + j * ld], y = S[q + j * ld];
-                S[p + j * ld] = c * x - s * y;
-                S[q + j * ld] = s * x + c * y;
+            // 2x2 blocks: rows of pair bi, columns of pair bj
+            for (int w = tid; w < half * half; w += nt) {
+                const int bi = w % half, bj = w / half;
+                const double si = sn_[bi], sj = sn_[bj];
+                if (si == 0.0 && sj == 0.0) continue;
+                const double ci = cs_[bi], cj = cs_[bj];
+                const int p = pp_[bi], q = qq_[bi], u = pp_[bj], v = qq_[bj];
+                const double m00 = S[p + u * ld], m01 = S[p + v * ld], m10 = S[q + u * ld], m11 = S[q + v * ld];
+                // rows: [c -s; s c] M
+                const double r00 = ci * m00 - si * m10, r01 = ci * m01 - si * m11;
+                const double r10 = si * m00 + ci * m10, r11 = si * m01 + ci * m11;
+                // columns: R [c s; -s c]
+                double n00 = cj * r00 - sj * r01, n01 = sj * r00 + cj * r01;
+                double n10 = cj * r10 - sj * r11, n11 = sj * r10 + cj * r11;
+                if (bi == bj) {  // the rotated pair itself: zero by construction
+                    n01 = 0.0;
+                    n10 = 0.0;
+                }
+                S[p + u * ld] = n00;
+                S[p + v * ld] = n01;
+                S[q + u * ld] = n10;
+                S[q + v * ld] = n11;
             }
-            __syncthreads();
-            // columns p, q  <- A P ;  V <- V P
+            // V <- V J (columns of each rotated pair)
             for (int w = tid; w < half * n; w += nt) {
-                const int i = w % half, j = w / half;
-                const int p = pp_[i], q = qq_[i];
-                const double c = cs_[i], s = sn_[i];
+                const int i = w / n, j = w % n;
+                const double s = sn_[i];
                 if (s == 0.0) continue;
-                const double x = S[j + p * ld], y = S[j + q * ld];
-                S[j + p * ld] = c * x - s * y;
-                S[j + q * ld] = s * x + c * y;
+                const double c = cs_[i];
+                const int p = pp_[i], q = qq_[i];
                 const double vx = V[j + (int64_t)p * n], vy = V[j + (int64_t)q * n];
                 V[j + (int64_t)p * n] = c * vx - s * vy;
                 V[j + (int64_t)q * n] = s * vx + c * vy;
             }
             __syncthreads();
         }
+        const bool any = rotated != 0;
+        __syncthreads();
+        if (tid == 0) rotated = 0;
+        if (!any) break;
+        __syncthreads();
     }
+    __syncthreads();
     for (int i = tid; i < n; i += nt) vals[i] = S[i + i * ld];
+    for (int w = tid; w < n_in * n_in; w += nt) Vout[w] = V[(w % n_in) + (int64_t)(w / n_in) * n];
     if (tid == 0 && sweeps_out) *sweeps_out = sweep;
 }
 
-int jacobi(const double *A, int n_in, double *V, double *vals, int *sweeps, cudaStream_t st) {
+// V: n_in x n_in eigenvectors (col-major); Vwork: (n_in+1)^2 doubles of
+// global scratch, used when the rotations do not fit in shared memory.
+int jacobi(const double *A, int n_in, double *Vwork, double *V, double *vals, int *sweeps, cudaStream_t st) {
     const int n = n_in + (n_in & 1);
     CREST_REQUIRE(n <= kJacobiMax, CREST_EINVAL, "Jacobi size %d exceeds %d", n, kJacobiMax);
-    const size_t smem = sizeof(double) * (size_t)n * (size_t)(n + 1);
-    CREST_CUDA_TRY(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     prof::Scope ps("eig_jacobi", st);
-    k_jacobi<<<1, 1024, smem, st>>>(A, n_in, n, V, vals, 40, sweeps);
+    if (n <= kJacobiSmemV) {
+        const size_t smem = sizeof(double) * ((size_t)n * (n + 1) + (size_t)n * n);
+        CREST_CUDA_TRY(cudaFuncSetAttribute(k_jacobi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_jacobi<true><<<1, 1024, smem, st>>>(A, n_in, n, nullptr, V, vals, 40, sweeps);
+    } else {
+        const size_t smem = sizeof(double) * (size_t)n * (size_t)(n + 1);
+        CREST_CUDA_TRY(cudaFuncSetAttribute(k_jacobi<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_jacobi<false><<<1, 1024, smem, st>>>(A, n_in, n, Vwork, V, vals, 40, sweeps);
+    }
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
 }
@@ -342,30 +395,35 @@ __global__ void k_random_block(double *V, int64_t n, uint64_t seed) {
     if (i < n) V[i] = (double)(mix64(seed ^ (uint64_t)i) >> 11) * 0x1.0p-52 - 1.0;
 }
 
-// Classical Gram-Schmidt with one re-orthogonalisation pass, one CTA,
-// column-major d x p block.  A column whose norm collapses below 1e-10 of
-// its starting norm is replaced by a deterministic random vector and
-// processed again.
-__global__ void __launch_bounds__(1024) k_cgs2(double *Q, int64_t d, int p, uint64_t seed, int *n_replaced) {
+// Block reduction helper (sum over the CTA), result valid in every thread.
+__device__ double block_sum(double v, double *red) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += red[w];
+    return s;
+}
+
+// Classical Gram-Schmidt with one re-orthogonalisation pass, one CTA, on
+// columns [j0, p) of a column-major d x p block (columns < j0 are already
+// orthonormal).  A column whose norm collapses below 1e-10 of its starting
+// norm is replaced by a deterministic random vector and processed again.
+// Fallback orthonormalisation when Cholesky QR meets a rank-deficient block.
+__global__ void __launch_bounds__(1024) k_cgs2(double *Q, int64_t d, int j0, int p, uint64_t seed) {
     extern __shared__ double sh[];  // r[p] + red[32]
     double *rcoef = sh;
     double *red = sh + p;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
-    int replaced = 0;
-    for (int j = 0; j < p; ++j) {
+    for (int j = j0; j < p; ++j) {
         double *y = Q + (int64_t)j * d;
         for (int attempt = 0; attempt < 3; ++attempt) {
-            // starting norm
             double s = 0.0;
             for (int64_t r = tid; r < d; r += nt) s += y[r] * y[r];
-            for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) red[wid] = s;
-            __syncthreads();
-            double n0 = 0.0;
-            for (int w = 0; w < nw; ++w) n0 += red[w];
-            __syncthreads();
+            const double n0 = block_sum(s, red);
             for (int pass = 0; pass < 2; ++pass) {
-                // r_i = q_i . y for i < j  (warp per i)
                 for (int i = wid; i < j; i += nw) {
                     const double *qi = Q + (int64_t)i * d;
                     double t = 0.0;
@@ -383,20 +441,13 @@ __global__ void __launch_bounds__(1024) k_cgs2(double *Q, int64_t d, int p, uint
             }
             s = 0.0;
             for (int64_t r = tid; r < d; r += nt) s += y[r] * y[r];
-            for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == 0) red[wid] = s;
-            __syncthreads();
-            double n1 = 0.0;
-            for (int w = 0; w < nw; ++w) n1 += red[w];
-            __syncthreads();
+            const double n1 = block_sum(s, red);
             if (n1 > 1e-20 * n0 && n1 > 0.0) {
                 const double inv = 1.0 / sqrt(n1);
                 for (int64_t r = tid; r < d; r += nt) y[r] *= inv;
                 __syncthreads();
                 break;
             }
-            // deficient: draw a fresh direction and retry
-            ++replaced;
             for (int64_t r = tid; r < d; r += nt)
                 y[r] = (double)(mix64(seed ^ ((uint64_t)(j * 7 + attempt + 1) << 40) ^ (uint64_t)r) >> 11) *
                            0x1.0p-52 -
@@ -404,12 +455,75 @@ __global__ void __launch_bounds__(1024) k_cgs2(double *Q, int64_t d, int p, uint
             __syncthreads();
         }
     }
-    if (tid == 0 && n_replaced) *n_replaced = replaced;
 }
 
-// r_i = || W_i - theta_i V_i || for i < k; out = max_i r_i (one block per column)
+// Cholesky QR factor for a block Y with Gram matrix B = Y^T Y (p x p).  The
+// Gram matrix is first equilibrated, B' = D B D with D = diag(B)^-1/2 (column
+// scaling leaves the span unchanged and removes the norm disparity a
+// Chebyshev filter creates), shifted by shift_coef * ||B'||_2 (bounded by
+// trace(B') = p), and factored B' = L L^T.  Rinv = D L^-T (upper triangular),
+// so Y Rinv has orthonormal columns.  One CTA, L and L^-1 in shared memory.
+// *fail = 1 when a column is zero or a pivot is not positive.
+__global__ void __launch_bounds__(1024) k_chol_inv(const double *__restrict__ B, int p, double shift_coef,
+                                                   double *__restrict__ Rinv, int *fail) {
+    extern __shared__ double sm[];
+    double *L = sm;                    // p x p, col-major
+    double *X = sm + (size_t)p * p;    // L^-1, col-major
+    __shared__ double dsc[kJacobiMax];
+    __shared__ int bad;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (tid == 0) bad = 0;
+    __syncthreads();
+    for (int i = tid; i < p; i += nt) {
+        const double b = B[i + (int64_t)i * p];
+        if (!(b > 0.0)) bad = 1;
+        dsc[i] = b > 0.0 ? 1.0 / sqrt(b) : 1.0;
+    }
+    __syncthreads();
+    const double shift = shift_coef * (double)p;
+    for (int w = tid; w < p * p; w += nt) {
+        const int r = w % p, c = w / p;
+        L[w] = (r == c) ? 1.0 + shift : B[w] * dsc[r] * dsc[c];
+        X[w] = 0.0;
+    }
+    __syncthreads();
+    for (int k = 0; k < p; ++k) {
+        if (tid == 0) {
+            const double dk = L[k + k * p];
+            if (!(dk > 0.0)) bad = 1;
+            L[k + k * p] = dk > 0.0 ? sqrt(dk) : 1.0;
+        }
+        __syncthreads();
+        const double lkk = L[k + k * p];
+        for (int i = k + 1 + tid; i < p; i += nt) L[i + k * p] /= lkk;
+        __syncthreads();
+        const int m = p - k - 1;
+        for (int w = tid; w < m * m; w += nt) {
+            const int i = k + 1 + w % m, j = k + 1 + w / m;
+            if (i >= j) L[i + j * p] -= L[i + k * p] * L[j + k * p];
+        }
+        __syncthreads();
+    }
+    // X = L^-1 by forward substitution, one column per thread
+    for (int c = tid; c < p; c += nt) {
+        for (int i = c; i < p; ++i) {
+            double v = (i == c) ? 1.0 : 0.0;
+            for (int k = c; k < i; ++k) v -= L[i + k * p] * X[k + c * p];
+            X[i + c * p] = v / L[i + i * p];
+        }
+    }
+    __syncthreads();
+    // Rinv = D (L^-1)^T
+    for (int w = tid; w < p * p; w += nt) {
+        const int r = w % p, c = w / p;
+        Rinv[w] = dsc[r] * X[c + r * p];
+    }
+    if (tid == 0 && bad) *fail = 1;
+}
+
+// r_i = || W_i - theta_i V_i || for the given columns; rmax[i] per column.
 __global__ void k_residual(const double *__restrict__ W, const double *__restrict__ V, const double *theta,
-                           int64_t d, double *out) {
+                           int64_t d, double *res) {
     __shared__ double red[32];
     const int i = blockIdx.x;
     const double th = theta[i];
@@ -418,14 +532,8 @@ __global__ void k_residual(const double *__restrict__ W, const double *__restric
         const double e = W[(int64_t)i * d + r] - th * V[(int64_t)i * d + r];
         s += e * e;
     }
-    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-        atomicMax(reinterpret_cast<unsigned long long *>(out), (unsigned long long)__double_as_longlong(sqrt(t)));
-    }
+    const double t = block_sum(s, red);
+    if (threadIdx.x == 0) res[i] = sqrt(t);
 }
 
 // Permute the Ritz basis: dst[:, j] = src[:, perm[j]] for j < p.
@@ -434,6 +542,13 @@ __global__ void k_permute_cols(const double *src, double *dst, int64_t d, const 
     if (idx >= d * p) return;
     const int64_t r = idx % d, j = idx / d;
     dst[idx] = src[(int64_t)perm[j] * d + r];
+}
+
+// Z[:, j] = (theta[j] - t) V[:, j] for j < nl (d x nl, col-major).
+__global__ void k_scale_cols(const double *V, const double *theta, double t, int64_t d, int nl, double *Z) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= d * nl) return;
+    Z[idx] = (theta[idx / d] - t) * V[idx];
 }
 
 // Symmetrise a p x p col-major matrix in place: H = (H + H^T)/2.
@@ -448,9 +563,120 @@ __global__ void k_symmetrise(double *H, int p) {
     }
 }
 
+// y = C x for a symmetric d x d C (column-major; reads column i for y_i).
+__global__ void k_symv(const double *__restrict__ C, int64_t d, const double *__restrict__ x, double *__restrict__ y) {
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= d) return;
+    const double *col = C + i * d;
+    double s = 0.0;
+    for (int64_t j = lane; j < d; j += 32) s += col[j] * x[j];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) y[i] = s;
+}
+
+// One Lanczos step after w = C v_j: alpha_j = v_j.w, w -= alpha v_j + beta v_{j-1},
+// full re-orthogonalisation (twice) against V[:, 0..j], beta_j = |w|,
+// v_{j+1} = w / beta_j.  One CTA; V is d x (kLanczos + 1) col-major.
+__global__ void __launch_bounds__(1024) k_lanczos_step(double *V, int64_t d, int j, double *w, double *ab) {
+    __shared__ double red[32];
+    __shared__ double coef[kLanczos + 1];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+    const double *vj = V + (int64_t)j * d;
+    double s = 0.0;
+    for (int64_t r = tid; r < d; r += nt) s += vj[r] * w[r];
+    const double alpha = block_sum(s, red);
+    const double beta_prev = j > 0 ? ab[kLanczos + j - 1] : 0.0;
+    for (int64_t r = tid; r < d; r += nt) {
+        double v = w[r] - alpha * vj[r];
+        if (j > 0) v -= beta_prev * V[(int64_t)(j - 1) * d + r];
+        w[r] = v;
+    }
+    __syncthreads();
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int i = wid; i <= j; i += nw) {
+            const double *qi = V + (int64_t)i * d;
+            double t = 0.0;
+            for (int64_t r = lane; r < d; r += 32) t += qi[r] * w[r];
+            for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (lane == 0) coef[i] = t;
+        }
+        __syncthreads();
+        for (int64_t r = tid; r < d; r += nt) {
+            double v = w[r];
+            for (int i = 0; i <= j; ++i) v -= coef[i] * V[(int64_t)i * d + r];
+            w[r] = v;
+        }
+        __syncthreads();
+    }
+    s = 0.0;
+    for (int64_t r = tid; r < d; r += nt) s += w[r] * w[r];
+    const double beta = sqrt(block_sum(s, red));
+    double *vn = V + (int64_t)(j + 1) * d;
+    const double inv = beta > 0.0 ? 1.0 / beta : 0.0;
+    for (int64_t r = tid; r < d; r += nt) vn[r] = w[r] * inv;
+    if (tid == 0) {
+        ab[j] = alpha;
+        ab[kLanczos + j] = beta;
+    }
+}
+
+// Lanczos tridiagonal T (L x L, col-major) from alpha = ab[0..L), beta = ab[kLanczos..).
+__global__ void k_tridiag(const double *ab, int L, double *T) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= L * L) return;
+    const int i = idx % L, j = idx / L;
+    T[idx] = (i == j) ? ab[i] : ((i == j + 1 || j == i + 1) ? ab[kLanczos + min(i, j)] : 0.0);
+}
+
 struct EigWork {
-    DevBuf C, V, W, Y0, Y1, H, Q, vals, sorted, perm, scal;
+    DevBuf C, V, W, Y0, Y1, H, Q, vals, sorted, perm, scal, lz, lw, lab, res, rinv, fail;
+    GemmWs g;
 };
+
+// Orthonormalise columns [j0, j0+q) of the d x p block Y against its first
+// j0 columns (already orthonormal) and among themselves: shifted Cholesky QR
+// passes (Fukaya et al. 2020), CGS2 on the device when Cholesky fails.
+int orthonormalise(EigWork &w, double *Y, int64_t d, int j0, int q, bool shifted, uint64_t seed, cudaStream_t st) {
+    const int D = (int)d;
+    double *Ya = Y + (int64_t)j0 * d;
+    double *T = w.Y1.as<double>();  // scratch d x p
+    double *B = w.H.as<double>();
+    double *Rinv = w.Q.as<double>();
+    int *fail = w.fail.as<int>();
+    const size_t csmem = sizeof(double) * 2 * (size_t)q * q;
+    CREST_CUDA_TRY(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem));
+    const int passes = shifted ? 3 : 2;
+    for (int pass = 0; pass < passes; ++pass) {
+        if (j0 > 0) {  // remove the locked directions (twice for orthogonality)
+            for (int rep = 0; rep < 2; ++rep) {
+                CREST_TRY(gemm(Gemm{j0, q, D, Y, D, 1, Ya, D, B, j0, 1.0, nullptr, 0.0, nullptr, 0.0}, w.g, st));
+                CREST_TRY(gemm(Gemm{D, q, j0, Y, D, 0, B, j0, Ya, D, -1.0, Ya, 1.0, nullptr, 0.0}, w.g, st));
+            }
+        }
+        CREST_TRY(gemm(Gemm{q, q, D, Ya, D, 1, Ya, D, B, q, 1.0, nullptr, 0.0, nullptr, 0.0}, w.g, st));
+        // shift = 11 (d q + q (q + 1)) u ||B'||_2 on the first pass of the shifted form
+        const double shift_coef = (shifted && pass == 0) ? 11.0 * ((double)d * q + (double)q * (q + 1)) * 0x1.0p-53 : 0.0;
+        CREST_CUDA_TRY(cudaMemsetAsync(fail, 0, sizeof(int), st));
+        {
+            prof::Scope ps("eig_cholqr", st);
+            k_chol_inv<<<1, 1024, csmem, st>>>(B, q, shift_coef, Rinv, fail);
+        }
+        CREST_CUDA_TRY(cudaGetLastError());
+        int hf = 0;
+        CREST_CUDA_TRY(cudaMemcpyAsync(&hf, fail, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CREST_CUDA_TRY(cudaStreamSynchronize(st));
+        if (hf) {
+            prof::Scope ps("eig_cgs2", st);
+            k_cgs2<<<1, 1024, sizeof(double) * (size_t)(j0 + q + 32), st>>>(Y, d, j0, j0 + q, seed + pass);
+            CREST_CUDA_TRY(cudaGetLastError());
+            return CREST_OK;
+        }
+        CREST_TRY(gemm(Gemm{D, q, q, Ya, D, 0, Rinv, q, T, D, 1.0, nullptr, 0.0, nullptr, 0.0}, w.g, st));
+        CREST_CUDA_TRY(cudaMemcpyAsync(Ya, T, sizeof(double) * (size_t)d * q, cudaMemcpyDeviceToDevice, st));
+    }
+    return CREST_OK;
+}
 
 }  // namespace
 
@@ -458,11 +684,18 @@ int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_
              double *out_vecs, double *out_total, EigStats *stats, cudaStream_t st) {
     CREST_REQUIRE(d >= 1 && n >= 2, CREST_ERUNTIME, "need at least 2 cells and 1 gene");
     CREST_REQUIRE(k >= 0 && k <= d, CREST_EINVAL, "k=%lld must be in [0, d=%lld]", (long long)k, (long long)d);
-    static thread_local EigWork w;
+    int dev = 0;
+    CREST_CUDA_TRY(cudaGetDevice(&dev));
+    CREST_REQUIRE(dev >= 0 && dev < 64, CREST_ERUNTIME, "device index %d out of range", dev);
+    static thread_local EigWork ws[64];  // per host thread and device
+    EigWork &w = ws[dev];
     const double nf = (double)n;
     CREST_TRY(w.C.ensure(sizeof(double) * (size_t)(d * d)));
     double *C = w.C.as<double>();
-    k_centre<<<(unsigned)ceil_div(d * d, 256), 256, 0, st>>>(G, colsum, d, nf, C);
+    {
+        prof::Scope ps("eig_centre", st);
+        k_centre<<<(unsigned)ceil_div(d * d, 256), 256, 0, st>>>(G, colsum, d, nf, C);
+    }
     CREST_CUDA_TRY(cudaGetLastError());
     k_trace<<<1, 32, 0, st>>>(C, d, out_total);
     CREST_CUDA_TRY(cudaGetLastError());
@@ -473,6 +706,8 @@ int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_
     CREST_TRY(w.sorted.ensure(sizeof(double) * 512));
     CREST_TRY(w.vals.ensure(sizeof(double) * 512));
     CREST_TRY(w.scal.ensure(sizeof(double) * 8));
+    CREST_TRY(w.res.ensure(sizeof(double) * 512));
+    CREST_TRY(w.fail.ensure(sizeof(int) * 4));
     int *perm = w.perm.as<int>();
     double *sorted = w.sorted.as<double>();
     double *jvals = w.vals.as<double>();
@@ -480,10 +715,11 @@ int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_
     if (d <= kJacobiMax) {  // whole matrix
         const int nn = (int)(d + (d & 1));
         CREST_TRY(w.Q.ensure(sizeof(double) * (size_t)nn * nn));
-        CREST_TRY(jacobi(C, (int)d, w.Q.as<double>(), jvals, w.perm.as<int>() + 256, st));
+        CREST_TRY(w.Y0.ensure(sizeof(double) * (size_t)nn * nn));
+        CREST_TRY(jacobi(C, (int)d, w.Y0.as<double>(), w.Q.as<double>(), jvals, w.perm.as<int>() + 256, st));
         k_rank<<<(unsigned)ceil_div(d, 128), 128, 0, st>>>(jvals, (int)d, perm, sorted);
         CREST_CUDA_TRY(cudaGetLastError());
-        k_emit<<<(unsigned)k, 256, 0, st>>>(w.Q.as<double>(), d, nn, perm, sorted, k, out_vals, out_vecs);
+        k_emit<<<(unsigned)k, 256, 0, st>>>(w.Q.as<double>(), d, d, perm, sorted, k, out_vals, out_vecs);
         CREST_CUDA_TRY(cudaGetLastError());
         if (stats) {
             int sweeps = 0;
@@ -495,10 +731,11 @@ int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_
     }
 
     int p = (int)round_up(k + 32, 16);
-    if (p > kJacobiMax) p = kJacobiMax;
+    if (p > kJacobiSmemV) p = kJacobiSmemV;
     if (p > d) p = (int)d;
     CREST_REQUIRE(k <= p - 8, CREST_EINVAL, "n_comps=%lld too large for the block eigensolver (max %d)",
-                  (long long)k, kJacobiMax - 8);
+                  (long long)k, kJacobiSmemV - 8);
+    const int D = (int)d;
     const size_t blk = sizeof(double) * (size_t)d * (size_t)p;
     CREST_TRY(w.V.ensure(blk));
     CREST_TRY(w.W.ensure(blk));
@@ -506,26 +743,58 @@ int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_
     CREST_TRY(w.Y1.ensure(blk));
     CREST_TRY(w.H.ensure(sizeof(double) * (size_t)p * p));
     CREST_TRY(w.Q.ensure(sizeof(double) * (size_t)p * p));
-    double *V = w.V.as<double>(), *W = w.W.as<double>(), *Y0 = w.Y0.as<double>(), *Y1 = w.Y1.as<double>();
+    CREST_TRY(w.lz.ensure(sizeof(double) * (size_t)d * (kLanczos + 1)));
+    CREST_TRY(w.lw.ensure(sizeof(double) * (size_t)d));
+    CREST_TRY(w.lab.ensure(sizeof(double) * 2 * kLanczos));
+    double *V = w.V.as<double>(), *W = w.W.as<double>(), *Y0 = w.Y0.as<double>();
     double *H = w.H.as<double>(), *Q = w.Q.as<double>();
-    double *scal = w.scal.as<double>();  // [0] gershgorin, [1] residual
-    const int D = (int)d;
-    const size_t cgs_smem = sizeof(double) * (size_t)(p + 32);
 
-    // spectrum bound
-    CREST_CUDA_TRY(cudaMemsetAsync(scal, 0, sizeof(double) * 2, st));
-    k_row_abs_max<<<256, 256, 0, st>>>(C, d, scal);
-    CREST_CUDA_TRY(cudaGetLastError());
-    double bound = 0.0;
-    CREST_CUDA_TRY(cudaMemcpyAsync(&bound, scal, sizeof(double), cudaMemcpyDeviceToHost, st));
-    // start block
-    k_random_block<<<(unsigned)ceil_div(d * p, 256), 256, 0, st>>>(V, d * p, 0x243f6a8885a308d3ull);
-    CREST_CUDA_TRY(cudaGetLastError());
-    k_cgs2<<<1, 1024, cgs_smem, st>>>(V, d, p, 0x13198a2e03707344ull, nullptr);
-    CREST_CUDA_TRY(cudaGetLastError());
-    CREST_CUDA_TRY(cudaStreamSynchronize(st));
-    if (!(bound > 0.0)) {
+    // ---- spectrum bounds by Lanczos (full re-orthogonalisation)
+    double lam_lo, lam_hi;
+    {
+        double *LZ = w.lz.as<double>(), *lw = w.lw.as<double>(), *lab = w.lab.as<double>();
+        k_random_block<<<(unsigned)ceil_div(d, 256), 256, 0, st>>>(LZ, d, 0x452821e638d01377ull);
+        CREST_CUDA_TRY(cudaGetLastError());
+        CREST_TRY(w.res.ensure(sizeof(double) * 512));
+        // normalise v0: one CGS2 pass over a single column
+        k_cgs2<<<1, 1024, sizeof(double) * 64, st>>>(LZ, d, 0, 1, 1);
+        CREST_CUDA_TRY(cudaGetLastError());
+        const int L = (int)std::min<int64_t>(kLanczos, d - 1);
+        {
+            prof::Scope ps("eig_lanczos", st);
+            for (int j = 0; j < L; ++j) {
+                k_symv<<<(unsigned)ceil_div(d * 32, 256), 256, 0, st>>>(C, d, LZ + (int64_t)j * d, lw);
+                k_lanczos_step<<<1, 1024, 0, st>>>(LZ, d, j, lw, lab);
+            }
+        }
+        CREST_CUDA_TRY(cudaGetLastError());
+        // Ritz values of T and the last components of its eigenvectors
+        k_tridiag<<<(unsigned)ceil_div(L * L, 256), 256, 0, st>>>(lab, L, H);
+        CREST_CUDA_TRY(cudaGetLastError());
+        CREST_TRY(jacobi(H, L, Y0, Q, jvals, nullptr, st));
+        std::vector<double> hab(2 * kLanczos), tw(L), tz((size_t)L * L);
+        CREST_CUDA_TRY(cudaMemcpyAsync(hab.data(), lab, sizeof(double) * 2 * kLanczos, cudaMemcpyDeviceToHost, st));
+        CREST_CUDA_TRY(cudaMemcpyAsync(tw.data(), jvals, sizeof(double) * L, cudaMemcpyDeviceToHost, st));
+        CREST_CUDA_TRY(cudaMemcpyAsync(tz.data(), Q, sizeof(double) * L * L, cudaMemcpyDeviceToHost, st));
+        CREST_CUDA_TRY(cudaStreamSynchronize(st));
+        int imin = 0, imax = 0;
+        for (int i = 1; i < L; ++i) {
+            if (tw[i] < tw[imin]) imin = i;
+            if (tw[i] > tw[imax]) imax = i;
+        }
+        const double bL = hab[kLanczos + L - 1];
+        const double rmin = fabs(bL * tz[(size_t)(L - 1) + (size_t)imin * L]);  // col-major
+        const double rmax = fabs(bL * tz[(size_t)(L - 1) + (size_t)imax * L]);
+        lam_hi = tw[imax] + rmax;
+        // a guard below the smallest Ritz value: eigenvalues a little below
+        // the damped interval only slow convergence, they cannot be chosen
+        lam_lo = tw[imin] - rmin - 1e-3 * (tw[imax] - tw[imin]);
+        if (lam_lo < 0.0) lam_lo = 0.0 - 1e-12 * fabs(lam_hi);
+    }
+    if (!(lam_hi > 0.0)) {
         // zero covariance: every eigenvalue is 0; any orthonormal basis will do
+        k_random_block<<<(unsigned)ceil_div(d * p, 256), 256, 0, st>>>(V, d * p, 0x243f6a8885a308d3ull);
+        k_cgs2<<<1, 1024, sizeof(double) * (size_t)(p + 32), st>>>(V, d, 0, p, 3);
         std::vector<int> hp(k);
         std::vector<double> hz(k, 0.0);
         for (int64_t i = 0; i < k; ++i) hp[i] = (int)i;
@@ -537,88 +806,110 @@ int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_
         return CREST_OK;
     }
 
+    // ---- start block
+    k_random_block<<<(unsigned)ceil_div(d * p, 256), 256, 0, st>>>(V, d * p, 0x243f6a8885a308d3ull);
+    CREST_CUDA_TRY(cudaGetLastError());
+    CREST_TRY(orthonormalise(w, V, d, 0, p, false, 11, st));
+
     const double tol = 1e-11;
-    const int max_outer = 80, degree = 12;
-    std::vector<double> theta(p);
-    int it = 0;
-    double res = INFINITY;
+    const int max_outer = 60;
+    std::vector<double> theta(p), hres(p);
+    int locked = 0, it = 0;
+    double res_max = INFINITY;
     bool converged = false;
     for (; it < max_outer; ++it) {
-        // Rayleigh-Ritz: W = C V, H = V^T W, H = Q diag(theta) Q^T
-        CREST_TRY(gemm(Gemm{D, p, D, C, D, 0, V, D, W, D, 1.0, nullptr, 0.0, nullptr, 0.0}, st));
-        CREST_TRY(gemm(Gemm{p, p, D, V, D, 1, W, D, H, p, 1.0, nullptr, 0.0, nullptr, 0.0}, st));
-        k_symmetrise<<<(unsigned)ceil_div(p * p, 256), 256, 0, st>>>(H, p);
+        const int q = p - locked;
+        double *Va = V + (int64_t)locked * d, *Wa = W + (int64_t)locked * d;
+        // Rayleigh-Ritz on the active columns: Wa = C Va, H = Va^T Wa
+        CREST_TRY(gemm(Gemm{D, q, D, C, D, 0, Va, D, Wa, D, 1.0, nullptr, 0.0, nullptr, 0.0}, w.g, st));
+        CREST_TRY(gemm(Gemm{q, q, D, Va, D, 1, Wa, D, H, q, 1.0, nullptr, 0.0, nullptr, 0.0}, w.g, st));
+        k_symmetrise<<<(unsigned)ceil_div(q * q, 256), 256, 0, st>>>(H, q);
         CREST_CUDA_TRY(cudaGetLastError());
-        CREST_TRY(jacobi(H, p, Q, jvals, nullptr, st));
-        k_rank<<<(unsigned)ceil_div(p, 128), 128, 0, st>>>(jvals, p, perm, sorted);
+        CREST_TRY(jacobi(H, q, Y0, Q, jvals, nullptr, st));
+        k_rank<<<(unsigned)ceil_div(q, 128), 128, 0, st>>>(jvals, q, perm, sorted + locked);
         CREST_CUDA_TRY(cudaGetLastError());
-        // V <- V Q_sorted, W <- W Q_sorted  (Q permuted into Y0 first)
-        k_permute_cols<<<(unsigned)ceil_div(p * p, 256), 256, 0, st>>>(Q, H, p, perm, p);
+        k_permute_cols<<<(unsigned)ceil_div(q * q, 256), 256, 0, st>>>(Q, H, q, perm, q);
         CREST_CUDA_TRY(cudaGetLastError());
-        CREST_TRY(gemm(Gemm{D, p, p, V, D, 0, H, p, Y0, D, 1.0, nullptr, 0.0, nullptr, 0.0}, st));
-        CREST_TRY(gemm(Gemm{D, p, p, W, D, 0, H, p, Y1, D, 1.0, nullptr, 0.0, nullptr, 0.0}, st));
-        std::swap(V, Y0);
-        std::swap(W, Y1);
-        // residuals of the wanted pairs
-        CREST_CUDA_TRY(cudaMemsetAsync(scal + 1, 0, sizeof(double), st));
-        k_residual<<<(unsigned)k, 256, 0, st>>>(W, V, sorted, d, scal + 1);
+        CREST_TRY(gemm(Gemm{D, q, q, Va, D, 0, H, q, Y0, D, 1.0, nullptr, 0.0, nullptr, 0.0}, w.g, st));
+        CREST_CUDA_TRY(cudaMemcpyAsync(Va, Y0, sizeof(double) * (size_t)d * q, cudaMemcpyDeviceToDevice, st));
+        CREST_TRY(gemm(Gemm{D, q, q, Wa, D, 0, H, q, Y0, D, 1.0, nullptr, 0.0, nullptr, 0.0}, w.g, st));
+        CREST_CUDA_TRY(cudaMemcpyAsync(Wa, Y0, sizeof(double) * (size_t)d * q, cudaMemcpyDeviceToDevice, st));
+        k_residual<<<(unsigned)q, 256, 0, st>>>(Wa, Va, sorted + locked, d, w.res.as<double>() + locked);
         CREST_CUDA_TRY(cudaGetLastError());
         CREST_CUDA_TRY(cudaMemcpyAsync(theta.data(), sorted, sizeof(double) * p, cudaMemcpyDeviceToHost, st));
-        double rmax = 0.0;
-        CREST_CUDA_TRY(cudaMemcpyAsync(&rmax, scal + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+        CREST_CUDA_TRY(cudaMemcpyAsync(hres.data(), w.res.as<double>(), sizeof(double) * p, cudaMemcpyDeviceToHost, st));
         CREST_CUDA_TRY(cudaStreamSynchronize(st));
         const double scale_ref = fmax(fabs(theta[0]), 1e-300);
-        res = rmax / scale_ref;
-        if (res <= tol) {
+        // lock the leading converged pairs (in order) and deflate them: their
+        // eigenvalues move to lam_lo, the edge of every damped interval, so
+        // the filter never amplifies what leaks back into the active block
+        const int l0 = locked;
+        while (locked < k && hres[locked] <= tol * scale_ref) ++locked;
+        if (locked > l0 && locked < k) {
+            const int nl = locked - l0;
+            double *Vl = V + (int64_t)l0 * d;
+            k_scale_cols<<<(unsigned)ceil_div(d * nl, 256), 256, 0, st>>>(Vl, sorted + l0, lam_lo, d, nl, Y0);
+            CREST_CUDA_TRY(cudaGetLastError());
+            Gemm g{D, D, nl, Y0, D, 0, Vl, D, C, D, -1.0, C, 1.0, nullptr, 0.0};
+            g.tB = 1;
+            CREST_TRY(gemm(g, w.g, st));
+        }
+        res_max = 0.0;
+        for (int i = 0; i < k; ++i) res_max = fmax(res_max, hres[i] / scale_ref);
+        if (locked >= k) {
             converged = true;
             break;
         }
         if (it + 1 >= max_outer) break;
-        // Chebyshev filter damping [lo, a], a = smallest Ritz value, reference point theta_0
-        const double a = theta[p - 1], lo = -1e-12 * bound;
-        if (!(a > lo) || !(theta[0] > a)) {
-            // no usable gap estimate: plain subspace iteration step
-            std::swap(V, W);
+        // Chebyshev filter on the active columns, damping [lam_lo, a]
+        const int qa = p - locked;
+        Va = V + (int64_t)locked * d;
+        Wa = W + (int64_t)locked * d;
+        const double a = theta[p - 1], top = theta[locked];
+        const double e = 0.5 * (a + lam_lo), c = 0.5 * (a - lam_lo);
+        if (!(c > 0.0) || !(top > a)) {
+            // no usable interval: one power step
+            CREST_CUDA_TRY(cudaMemcpyAsync(Va, Wa, sizeof(double) * (size_t)d * qa, cudaMemcpyDeviceToDevice, st));
         } else {
-            const double e = 0.5 * (a + lo), c = 0.5 * (a - lo);
-            const double sigma1 = c / (theta[0] - e);
+            // degree: growth 2e4 of the weakest wanted value over the damped
+            // interval, capped so that no eigenvalue of the active operator
+            // grows by more than 1e8 (the filtered block stays within reach of
+            // shifted Cholesky QR).  Until a pair is locked the largest
+            // eigenvalue is bounded by the Lanczos estimate, afterwards by the
+            // leading active Ritz value plus its residual.
+            double bound = top + hres[locked];
+            if (locked == 0) bound = fmax(bound, lam_hi);
+            const double xk = (theta[k - 1] - e) / c, xb = (bound - e) / c;
+            const double gk = acosh(fmax(xk, 1.0 + 1e-12)), gb = acosh(fmax(xb, 1.0 + 1e-12));
+            int m = (int)ceil(log(2e4) / fmax(gk, 1e-6));
+            const int m_cap = (int)floor(log(1e8) / fmax(gb, 1e-6));
+            m = std::max(2, std::min(m, std::min(m_cap, 60)));
+            const double sigma1 = c / (top - e);
             double sigma = sigma1;
-            // Y0 = V (previous), Y1 = sigma1/c (C V - e V) = sigma1/c (W - e V)
-            // W already holds C V for the current V
-            {
-                // Y1 = (sigma1/c) * W + (-sigma1*e/c) * V
-                CREST_TRY(gemm(Gemm{D, p, 0, C, D, 0, V, D, Y1, D, 0.0, W, sigma1 / c, V, -sigma1 * e / c}, st));
-            }
-            double *Yprev = V, *Ycur = Y1, *Ynext = Y0;
-            for (int j = 2; j <= degree; ++j) {
+            double *Yprev = Va, *Ycur = w.Y1.as<double>(), *Ynext = Y0;
+            // Y1 = (sigma1/c) (C Va - e Va); Wa already holds C Va
+            CREST_TRY(gemm(Gemm{D, qa, 0, C, D, 0, Va, D, Ycur, D, 0.0, Wa, sigma1 / c, Va, -sigma1 * e / c}, w.g, st));
+            for (int j = 2; j <= m; ++j) {
                 const double sigma_next = 1.0 / (2.0 / sigma1 - sigma);
-                // Ynext = (2 sigma_next / c) (C Ycur - e Ycur) - sigma sigma_next Yprev
-                CREST_TRY(gemm(Gemm{D, p, D, C, D, 0, Ycur, D, Ynext, D, 2.0 * sigma_next / c, Ycur,
+                CREST_TRY(gemm(Gemm{D, qa, D, C, D, 0, Ycur, D, Ynext, D, 2.0 * sigma_next / c, Ycur,
                                     -2.0 * sigma_next * e / c, Yprev, -sigma * sigma_next},
-                               st));
+                               w.g, st));
                 sigma = sigma_next;
                 double *t = Yprev;
                 Yprev = Ycur;
                 Ycur = Ynext;
-                Ynext = t;
+                Ynext = (t == Va) ? w.W.as<double>() + (int64_t)locked * d : t;  // Va's storage is reused below
             }
-            // make V the filtered block (V, Y0, Y1 are all free except Ycur)
-            if (Ycur != V) {
-                CREST_CUDA_TRY(cudaMemcpyAsync(V, Ycur, blk, cudaMemcpyDeviceToDevice, st));
-            }
+            CREST_CUDA_TRY(cudaMemcpyAsync(Va, Ycur, sizeof(double) * (size_t)d * qa, cudaMemcpyDeviceToDevice, st));
         }
-        {
-            prof::Scope ps("eig_cgs2", st);
-            k_cgs2<<<1, 1024, cgs_smem, st>>>(V, d, p, 0x13198a2e03707344ull + (uint64_t)it, nullptr);
-        }
-        CREST_CUDA_TRY(cudaGetLastError());
+        CREST_TRY(orthonormalise(w, V, d, locked, qa, true, 1000 + it, st));
     }
-    if (stats) *stats = EigStats{it + 1, converged ? 1 : 0, res};
-    // sorted Ritz pairs are already in order: identity permutation
-    std::vector<int> ident(k);
-    for (int64_t i = 0; i < k; ++i) ident[i] = (int)i;
-    CREST_CUDA_TRY(cudaMemcpyAsync(perm, ident.data(), sizeof(int) * k, cudaMemcpyHostToDevice, st));
-    k_emit<<<(unsigned)k, 256, 0, st>>>(V, d, d, perm, sorted, k, out_vals, out_vecs);
+    if (stats) *stats = EigStats{it + 1, converged ? 1 : 0, res_max};
+    // V columns 0..k-1 are the wanted Ritz vectors: locked ones (descending,
+    // in locking order) then the active ones; order them by value once more
+    k_rank<<<(unsigned)ceil_div(k, 128), 128, 0, st>>>(sorted, (int)k, perm, jvals);
+    CREST_CUDA_TRY(cudaGetLastError());
+    k_emit<<<(unsigned)k, 256, 0, st>>>(V, d, d, perm, jvals, k, out_vals, out_vecs);
     CREST_CUDA_TRY(cudaGetLastError());
     CREST_CUDA_TRY(cudaStreamSynchronize(st));
     return CREST_OK;

@@ -50,20 +50,57 @@ __global__ void k_tile_shift(int precision, const double *__restrict__ bias, int
     shift[j] = v;
 }
 
+// ------------------------------------------------------------- HVG codes
+// code[g] for a store gene id g < n_gene_map: -1 when the gene is dropped,
+// sub_map[gene_map[g]] in [0, d) for an HVG column, d for another kept gene
+// (it still counts towards the cell total).  One table lookup per entry
+// then serves both the normalisation total and the HVG selection.
+__global__ void k_hvg_code(const int32_t *__restrict__ gene_map, int64_t n_gene_map,
+                           const int32_t *__restrict__ sub_map, int64_t n_vars, int64_t d, int32_t *__restrict__ code) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_gene_map) return;
+    const int32_t m = gene_map[g];
+    int32_t v = -1;
+    if (m >= 0) v = (m < n_vars && sub_map[m] >= 0) ? sub_map[m] : (int32_t)d;
+    code[g] = v;
+}
+
+int launch_hvg_code(const DevChunk &c, const int32_t *sub_map, int64_t n_vars, int64_t d, int32_t *code,
+                    cudaStream_t st) {
+    if (c.n_gene_map <= 0) return CREST_OK;
+    k_hvg_code<<<(unsigned)ceil_div(c.n_gene_map, 256), 256, 0, st>>>(c.gene_map, c.n_gene_map, sub_map, n_vars, d,
+                                                                      code);
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
+}
+
+// Shared-memory copy of the codes as int16 (d < 2^15 - 1) when it fits next
+// to the kernel's other buffers; the global int32 table otherwise.
+bool codes_in_smem(int64_t n_gene_map, int64_t d, size_t other_smem) {
+    return d < 32767 && other_smem + 2 * (size_t)round_up(n_gene_map, 8) <= (size_t)kMaxSmem;
+}
+
 // ------------------------------------------------------------- densify
-// Warp per cell row i of the tile (i < m_pad, padding rows included).  The
-// row is built in a per-warp shared-memory buffer -- the zero-entry value of
-// every gene (shift for kept cells, 0 for dropped / padding rows), then the
-// cell's stored HVG entries -- and written out with 16-byte stores, so the
-// densified tile costs one coalesced write per element.  The colsum of S
-// (FP32 / BF16X3) is privatised per block in shared memory.
+// Warp per cell row i of the tile (i < m_pad, padding rows included),
+// written straight into the (L2-resident) tile.  One read of the cell's
+// entries: lanes add up the kept values (the normalisation total) and queue
+// the HVG entries (code, raw value), in entry order, in a per-warp
+// shared-memory queue.  Then the row is filled with the zero-entry value of
+// every gene -- the shift for kept cells, 0 for dropped / padding rows --
+// with 16-byte stores and, after a warp barrier that orders the two sets of
+// stores, the queued entries are transformed and stored.  A cell with more
+// than kQueue HVG entries, or whose total needs the in-order fold, reads its
+// entries a second time.  The colsum of S (FP32 / BF16X3) is privatised per
+// block in shared memory.  Duplicate (cell, gene) entries are not supported
+// (one of them lands in the tile).
 template <int MODE>  // 0 FP64 (T = S), 1 FP32 (T = S + shift), 2 BF16X3 (hi/lo of S + shift)
 struct RowElem;
 template <> struct RowElem<0> { using T = double; };
 template <> struct RowElem<1> { using T = float; };
 template <> struct RowElem<2> { using T = __nv_bfloat16; };
 
-constexpr int kDensifyWarps = 8;
+constexpr int kDensifyWarps = 32;
+constexpr int kQueue = 256;
 
 // bf16 split of a tile value (hi + lo ~ z to 2^-17 relative).  hi may come
 // from a double rounding through f32: any nearby bf16 works, lo holds the rest.
@@ -73,76 +110,130 @@ __device__ __forceinline__ void split_bf16(double z, __nv_bfloat16 &hi, __nv_bfl
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kDensifyWarps * 32) k_densify(DevChunk c, const int32_t *__restrict__ sub_map,
-                                                               DevScale t, const double *__restrict__ shift,
-                                                               int64_t d, int64_t d_pad, int64_t m_pad, void *tile,
-                                                               double *__restrict__ colsum, int64_t *n_kept) {
+static size_t densify_smem_fixed(int64_t d, int64_t d_pad) {
+    using E = typename RowElem<MODE>::T;
+    const size_t priv = MODE != 0 ? sizeof(double) * (size_t)round_up(d, 2) + sizeof(E) * (size_t)d_pad : 0;
+    return priv + (size_t)kDensifyWarps * kQueue * (sizeof(int32_t) + sizeof(float));
+}
+
+template <int MODE, bool SMAP>
+__global__ void __launch_bounds__(kDensifyWarps * 32, 1) k_densify(DevChunk c, const int32_t *__restrict__ code,
+                                                                   DevScale t, const double *__restrict__ shift,
+                                                                   int64_t d, int64_t d_pad, int64_t m_pad,
+                                                                   void *tile, double *__restrict__ colsum,
+                                                                   int64_t *n_kept) {
     using E = typename RowElem<MODE>::T;
     extern __shared__ __align__(16) unsigned char smem[];
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int rows_per_warp = MODE == 2 ? 2 : 1;  // bf16: hi row then lo row
-    // [shift row (tile type)] [per-warp row buffers] [colsum of S (f64)]
-    E *shift_row = reinterpret_cast<E *>(smem);
-    E *row = shift_row + d_pad + (size_t)wid * rows_per_warp * d_pad;
-    double *s_col = reinterpret_cast<double *>(smem + sizeof(E) * (size_t)(1 + kDensifyWarps * rows_per_warp) * d_pad);
-    const bool priv = MODE != 0;
-    for (int64_t j = threadIdx.x; j < d_pad; j += blockDim.x) shift_row[j] = (E)((shift && j < d) ? shift[j] : 0.0);
-    if (priv)
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    constexpr bool priv = MODE != 0;
+    // [colsum of S (f64)] [shift row (tile type)]   (MODE != 0)
+    // [queue codes (int32)] [queue values (f32)] [codes (int16), SMAP]
+    double *s_col = reinterpret_cast<double *>(smem);
+    E *shift_row = reinterpret_cast<E *>(smem + (priv ? sizeof(double) * (size_t)round_up(d, 2) : 0));
+    unsigned char *qbase = reinterpret_cast<unsigned char *>(shift_row) + (priv ? sizeof(E) * (size_t)d_pad : 0);
+    int32_t *q_code = reinterpret_cast<int32_t *>(qbase) + (size_t)wid * kQueue;
+    float *q_x = reinterpret_cast<float *>(qbase + sizeof(int32_t) * (size_t)kDensifyWarps * kQueue) +
+                 (size_t)wid * kQueue;
+    int16_t *s_code = reinterpret_cast<int16_t *>(qbase + (sizeof(int32_t) + sizeof(float)) * (size_t)kDensifyWarps * kQueue);
+    if (priv) {
+        for (int64_t j = threadIdx.x; j < d_pad; j += blockDim.x) shift_row[j] = (E)((shift && j < d) ? shift[j] : 0.0);
         for (int64_t j = threadIdx.x; j < d; j += blockDim.x) s_col[j] = 0.0;
+    }
+    if (SMAP)
+        for (int64_t j = threadIdx.x; j < c.n_gene_map; j += blockDim.x) s_code[j] = (int16_t)code[j];
     __syncthreads();
+    auto lookup = [&](uint32_t g) -> int32_t { return SMAP ? (int32_t)s_code[g] : __ldg(code + g); };
+    const int32_t dd = (int32_t)d;
     const int64_t warp = (int64_t)blockIdx.x * kDensifyWarps + wid;
     const int64_t n_warps = (int64_t)gridDim.x * kDensifyWarps;
     const int64_t nvec = d_pad * (int64_t)sizeof(E) / 16;
+    E *hi_plane = reinterpret_cast<E *>(tile);
+    E *lo_plane = hi_plane + (size_t)m_pad * d_pad;  // BF16X3 only
+    const uint4 zero = make_uint4(0, 0, 0, 0);
+    const bool norm = c.target_sum > 0.0;
     int kept_count = 0;
     for (int64_t i = warp; i < m_pad; i += n_warps) {
         int64_t lo = 0, hi = 0, r = -1;
         if (i < c.n_spans) r = span_row(c, i, lo, hi);
         const bool kept = r >= 0;
-        // zero-entry value of each gene: the shift row (exact in the tile type) or 0
+        // one pass: total of the kept values and the queue of HVG entries
+        double tsum = 0.0;
+        bool ok = true, ovf = false;
+        int nq = 0;
+        if (kept) {
+            for_entries_by<8, false>(c, lo, hi, lookup, [&](int32_t m, float x) {
+                if (m >= 0 && norm) {
+                    ok = ok && small_integer((double)x);
+                    tsum += (double)x;
+                }
+                const bool hv = m >= 0 && m < dd;
+                const unsigned mask = __ballot_sync(kFull, hv);
+                if (!mask) return;
+                if (nq + __popc(mask) > kQueue) {
+                    ovf = true;
+                    return;
+                }
+                if (hv) {
+                    const int pos = nq + __popc(mask & ((1u << lane) - 1u));
+                    q_code[pos] = m;
+                    q_x[pos] = x;
+                }
+                nq += __popc(mask);
+            });
+        }
+        // fill the row with the zero-entry values
+        E *row = hi_plane + (size_t)i * d_pad;
         {
             uint4 *dst = reinterpret_cast<uint4 *>(row);
             const uint4 *src = reinterpret_cast<const uint4 *>(shift_row);
-            const uint4 zero = make_uint4(0, 0, 0, 0);
-            for (int64_t v = lane; v < nvec; v += 32) {
-                dst[v] = kept ? src[v] : zero;
-                if (MODE == 2) dst[nvec + v] = zero;
+            for (int64_t v = lane; v < nvec; v += 32) dst[v] = (priv && kept) ? src[v] : zero;
+            if (MODE == 2) {
+                uint4 *dlo = reinterpret_cast<uint4 *>(lo_plane + (size_t)i * d_pad);
+                for (int64_t v = lane; v < nvec; v += 32) dlo[v] = zero;
             }
         }
-        __syncwarp();
-        if (kept) {
-            kept_count += 1;
-            const double scale = cell_scale(c, lo, hi);
-            for_entries<4>(c, lo, hi, [&](int32_t m, float x) {
-                const int32_t sub = m >= 0 ? __ldg(sub_map + m) : -1;
-                if (sub < 0) return;
-                const double s = scale_value(t, sub, transform_value(c, scale, x));
-                if (MODE == 0) {
-                    row[sub] = s;
+        __syncwarp();  // orders the fill before the scattered entry stores; queue visible
+        if (!kept) continue;
+        kept_count += 1;
+        double scale = 1.0;
+        if (norm) {
+            double total;
+            if (__all_sync(kFull, ok)) {
+                total = warp_sum(tsum);
+            } else {
+                OrderedSum ts;
+                for_entries_by<4, false>(c, lo, hi, lookup,
+                                         [&](int32_t m, float x) { ts.add(m >= 0 ? (double)x : 0.0); });
+                total = ts.acc;
+            }
+            scale = total > 0.0 ? c.target_sum / total : 1.0;
+        }
+        E *row_lo = lo_plane + (size_t)i * d_pad;
+        auto put = [&](int32_t sub, float x) {
+            const double s = scale_value(t, sub, transform_value(c, scale, x));
+            if (MODE == 0) {
+                row[sub] = s;
+            } else {
+                const double z = shift ? __dadd_rn(s, __ldg(shift + sub)) : s;
+                if (MODE == 1) {
+                    row[sub] = (E)__double2float_rn(z);
                 } else {
-                    const double z = shift ? __dadd_rn(s, __ldg(shift + sub)) : s;
-                    if (MODE == 1) {
-                        row[sub] = (E)__double2float_rn(z);
-                    } else {
-                        __nv_bfloat16 h, l;
-                        split_bf16(z, h, l);
-                        row[sub] = h;
-                        row[d_pad + sub] = l;
-                    }
-                    atomicAdd(s_col + sub, s);
+                    __nv_bfloat16 h, l;
+                    split_bf16(z, h, l);
+                    row[sub] = h;
+                    row_lo[sub] = l;
                 }
+                atomicAdd(s_col + sub, s);
+            }
+        };
+        if (!ovf) {
+            for (int e = lane; e < nq; e += 32) put(q_code[e], q_x[e]);
+        } else {
+            for_entries_by<8, true>(c, lo, hi, lookup, [&](int32_t m, float x) {
+                if (m >= 0 && m < dd) put(m, x);
             });
         }
-        __syncwarp();
-        // coalesced 16-byte stores of the finished row(s)
-        const uint4 *src = reinterpret_cast<const uint4 *>(row);
-        uint4 *dst = reinterpret_cast<uint4 *>(reinterpret_cast<E *>(tile) + (size_t)i * d_pad);
-        for (int64_t v = lane; v < nvec; v += 32) dst[v] = src[v];
-        if (MODE == 2) {
-            uint4 *dst_lo = reinterpret_cast<uint4 *>(reinterpret_cast<E *>(tile) + (size_t)m_pad * d_pad +
-                                                      (size_t)i * d_pad);
-            for (int64_t v = lane; v < nvec; v += 32) dst_lo[v] = src[nvec + v];
-        }
-        __syncwarp();
+        __syncwarp();  // queue reuse
     }
     if (lane == 0 && kept_count) atomicAdd(reinterpret_cast<unsigned long long *>(n_kept), (unsigned long long)kept_count);
     if (priv) {
@@ -152,25 +243,32 @@ __global__ void __launch_bounds__(kDensifyWarps * 32) k_densify(DevChunk c, cons
     }
 }
 
-template <int MODE>
-static int launch_densify_t(const DevChunk &c, const int32_t *sub_map, const DevScale &t, const double *shift,
-                            const GramWork &w, int64_t m_pad, cudaStream_t st) {
-    using E = typename RowElem<MODE>::T;
-    const int rows_per_warp = MODE == 2 ? 2 : 1;
-    const size_t smem = sizeof(E) * (size_t)(1 + kDensifyWarps * rows_per_warp) * w.d_pad +
-                        (MODE != 0 ? sizeof(double) * (size_t)w.d : 0);
-    CREST_REQUIRE(smem <= 220 * 1024, CREST_EINVAL, "d=%lld too large for the densify row buffers", (long long)w.d);
-    CREST_CUDA_TRY(cudaFuncSetAttribute(k_densify<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+template <int MODE, bool SMAP>
+static int launch_densify_k(const DevChunk &c, const int32_t *code, const DevScale &t, const double *shift,
+                            const GramWork &w, int64_t m_pad, size_t smem, cudaStream_t st) {
+    CREST_CUDA_TRY(cudaFuncSetAttribute(k_densify<MODE, SMAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int64_t blocks = ceil_div(m_pad, kDensifyWarps);
-    const int64_t cap = (int64_t)device_sms() * 4;
+    const int64_t cap = (int64_t)device_sms();
     if (blocks > cap) blocks = cap;
-    k_densify<MODE><<<(unsigned)blocks, kDensifyWarps * 32, smem, st>>>(c, sub_map, t, shift, w.d, w.d_pad, m_pad,
-                                                                         w.tile, w.colsum_chunk, w.n_kept);
+    k_densify<MODE, SMAP><<<(unsigned)blocks, kDensifyWarps * 32, smem, st>>>(c, code, t, shift, w.d, w.d_pad, m_pad,
+                                                                               w.tile, w.colsum_chunk, w.n_kept);
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
 }
 
-int launch_densify(const DevChunk &c, const int32_t *sub_map, const DevScale &t, const GramWork &w,
+template <int MODE>
+static int launch_densify_t(const DevChunk &c, const int32_t *code, const DevScale &t, const double *shift,
+                            const GramWork &w, int64_t m_pad, cudaStream_t st) {
+    const size_t fixed = densify_smem_fixed<MODE>(w.d, w.d_pad);
+    CREST_REQUIRE(fixed <= (size_t)kMaxSmem, CREST_EINVAL, "d=%lld too large for the densify shared buffers",
+                  (long long)w.d);
+    if (codes_in_smem(c.n_gene_map, w.d, fixed))
+        return launch_densify_k<MODE, true>(c, code, t, shift, w, m_pad,
+                                            fixed + 2 * (size_t)round_up(c.n_gene_map, 8), st);
+    return launch_densify_k<MODE, false>(c, code, t, shift, w, m_pad, fixed, st);
+}
+
+int launch_densify(const DevChunk &c, const int32_t *code, const DevScale &t, const GramWork &w,
                    cudaStream_t st) {
     CREST_REQUIRE(c.n_spans <= w.m_cap, CREST_EINVAL, "tile holds %lld cells, chunk has %lld",
                   (long long)w.m_cap, (long long)c.n_spans);
@@ -184,9 +282,9 @@ int launch_densify(const DevChunk &c, const int32_t *sub_map, const DevScale &t,
         shift = w.shift;
     }
     prof::Scope ps("densify", st);
-    if (w.precision == CREST_GRAM_FP64) return launch_densify_t<0>(c, sub_map, t, nullptr, w, m_pad, st);
-    if (w.precision == CREST_GRAM_FP32) return launch_densify_t<1>(c, sub_map, t, shift, w, m_pad, st);
-    return launch_densify_t<2>(c, sub_map, t, shift, w, m_pad, st);
+    if (w.precision == CREST_GRAM_FP64) return launch_densify_t<0>(c, code, t, nullptr, w, m_pad, st);
+    if (w.precision == CREST_GRAM_FP32) return launch_densify_t<1>(c, code, t, shift, w, m_pad, st);
+    return launch_densify_t<2>(c, code, t, shift, w, m_pad, st);
 }
 
 // ------------------------------------------------------------ FP64 SYRK

@@ -32,32 +32,66 @@ __global__ void __launch_bounds__(256) k_qc(DevChunk c, const uint8_t *__restric
             continue;
         }
         const bool tf = c.target_sum > 0.0 || c.log1p;
-        const double scale = tf ? cell_scale(c, lo, hi) : 1.0;
-        OrderedSum t, f;
+        double t_acc = 0.0, f_acc = 0.0;
         uint32_t n = 0;
-        for_entries<4>(c, lo, hi, [&](int32_t m, float x) {
-            const float v = (tf && m >= 0) ? transform_value(c, scale, x) : x;
-            const bool nz = m >= 0 && v != 0.0f;
-            const bool fl = nz && flag[m];
-            t.add(nz ? (double)v : 0.0);
-            f.add(fl ? (double)v : 0.0);
-            n += __popc(__ballot_sync(kFull, nz));
-            if (nz) {
+        if (!tf) {
+            // raw values: lane-private sums, exact (hence order-free) when
+            // every non-zero value is an integer below 2^24
+            double ts = 0.0, fs = 0.0;
+            bool ok = true;
+            for_entries<8>(c, lo, hi, [&](int32_t m, float x) {
+                if (m < 0 || x == 0.0f) return;
+                const double v = (double)x;
+                ok = ok && small_integer(v);
+                ts += v;
+                if (flag[m]) fs += v;
+                n += 1;
                 atomicAdd(gene_ncells + m, 1u);
-                atomicAdd(gene_total + m, (double)v);
+                atomicAdd(gene_total + m, v);
+            });
+            n = __reduce_add_sync(kFull, n);
+            if (__all_sync(kFull, ok)) {
+                t_acc = warp_sum(ts);
+                f_acc = warp_sum(fs);
+            } else {  // in entry order
+                OrderedSum t, f;
+                for_entries<4>(c, lo, hi, [&](int32_t m, float x) {
+                    const bool nz = m >= 0 && x != 0.0f;
+                    t.add(nz ? (double)x : 0.0);
+                    f.add(nz && flag[m] ? (double)x : 0.0);
+                });
+                t_acc = t.acc;
+                f_acc = f.acc;
             }
-        });
+        } else {
+            const double scale = cell_scale(c, lo, hi);
+            OrderedSum t, f;
+            for_entries<4>(c, lo, hi, [&](int32_t m, float x) {
+                const float v = m >= 0 ? transform_value(c, scale, x) : x;
+                const bool nz = m >= 0 && v != 0.0f;
+                const bool fl = nz && flag[m];
+                t.add(nz ? (double)v : 0.0);
+                f.add(fl ? (double)v : 0.0);
+                n += __popc(__ballot_sync(kFull, nz));
+                if (nz) {
+                    atomicAdd(gene_ncells + m, 1u);
+                    atomicAdd(gene_total + m, (double)v);
+                }
+            });
+            t_acc = t.acc;
+            f_acc = f.acc;
+        }
         if (lane == 0) {
             if (span_row_out) {
                 span_row_out[i] = row;
-                span_t[i] = t.acc;
+                span_t[i] = t_acc;
                 span_n[i] = n;
-                span_f[i] = f.acc;
+                span_f[i] = f_acc;
             }
             if (row_t) {
-                atomicAdd(row_t + row, t.acc);
+                atomicAdd(row_t + row, t_acc);
                 atomicAdd(row_n + row, n);
-                atomicAdd(row_f + row, f.acc);
+                atomicAdd(row_f + row, f_acc);
             }
         }
     }
@@ -73,7 +107,7 @@ __global__ void __launch_bounds__(256) k_gene_stats(DevChunk c, double *__restri
         int64_t lo, hi;
         if (span_row(c, i, lo, hi) < 0) continue;
         const double scale = cell_scale(c, lo, hi);
-        for_entries<4>(c, lo, hi, [&](int32_t m, float x) {
+        for_entries<8>(c, lo, hi, [&](int32_t m, float x) {
             if (m < 0) return;
             const double v = (double)transform_value(c, scale, x);
             const double ev = expm1(v);
@@ -90,40 +124,137 @@ __global__ void __launch_bounds__(256) k_gene_stats(DevChunk c, double *__restri
 // -------------------------------------------------------------- project (K6)
 // src/kernels.rs:352-371.  For each kept cell: a[j] = sum over HVG entries
 // (entry order) of s * V[sub, j] in f64 without fusing; out[row, j] += (f32)a[j].
-// Lane l owns components l, l+32, ... (k <= 128).
-template <int KPL>
-__global__ void __launch_bounds__(256) k_project(DevChunk c, const int32_t *__restrict__ sub_map, DevScale t,
-                                                 const double *__restrict__ V, int k, float *__restrict__ out,
-                                                 int by_span) {
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    const int lane = lane_id();
+// Lane l owns components l, l+32, ... (k <= 128).  One read of the cell's
+// entries forms the normalisation total and queues the HVG entries (code,
+// raw value) in entry order in a per-warp shared-memory queue; once the
+// scale is known the queued values are transformed in parallel, and the
+// queue is consumed U entries at a time with all V-row loads issued before
+// the U ordered additions, so the L2 latency of the V gathers overlaps.  A
+// cell with more than kProjQueue HVG entries (or whose total needs the
+// in-order fold) reads its entries again.
+constexpr int kProjWarps = 32;
+constexpr int kProjQueue = 256;
+constexpr size_t kProjSmemFixed = (size_t)kProjWarps * kProjQueue * (sizeof(int32_t) + sizeof(float) + sizeof(double));
+
+template <int KPL, bool SMAP>
+__global__ void __launch_bounds__(kProjWarps * 32, 1) k_project(DevChunk c, const int32_t *__restrict__ code,
+                                                                int32_t d, DevScale t, const double *__restrict__ V,
+                                                                int k, float *__restrict__ out, int by_span) {
+    constexpr int U = KPL >= 4 ? 4 : 8;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int wid = threadIdx.x >> 5, lane = lane_id();
+    double *q_val = reinterpret_cast<double *>(smem) + (size_t)wid * kProjQueue;
+    int32_t *q_code = reinterpret_cast<int32_t *>(smem + sizeof(double) * kProjWarps * kProjQueue) +
+                      (size_t)wid * kProjQueue;
+    float *q_x = reinterpret_cast<float *>(smem + (sizeof(double) + sizeof(int32_t)) * kProjWarps * kProjQueue) +
+                 (size_t)wid * kProjQueue;
+    int16_t *s_code = reinterpret_cast<int16_t *>(smem + kProjSmemFixed);
+    if (SMAP)
+        for (int64_t j = threadIdx.x; j < c.n_gene_map; j += blockDim.x) s_code[j] = (int16_t)code[j];
+    __syncthreads();
+    auto lookup = [&](uint32_t g) -> int32_t { return SMAP ? (int32_t)s_code[g] : __ldg(code + g); };
+    const int64_t warp = (int64_t)blockIdx.x * kProjWarps + wid;
+    const int64_t n_warps = (int64_t)gridDim.x * kProjWarps;
+    const bool norm = c.target_sum > 0.0;
     for (int64_t i = warp; i < c.n_spans; i += n_warps) {
         int64_t lo, hi;
         const int64_t row = span_row(c, i, lo, hi);
         if (row < 0) continue;
-        const double scale = cell_scale(c, lo, hi);
         double acc[KPL];
 #pragma unroll
         for (int q = 0; q < KPL; ++q) acc[q] = 0.0;
-        for_entries<2>(c, lo, hi, [&](int32_t m, float x) {
-            const int32_t sub = m >= 0 ? __ldg(sub_map + m) : -1;
-            double s = 0.0;
-            if (sub >= 0) s = scale_value(t, sub, transform_value(c, scale, x));
-            unsigned mask = __ballot_sync(kFull, sub >= 0);
-            while (mask) {
-                const int src = __ffs(mask) - 1;
-                mask &= mask - 1;
-                const int32_t sj = __shfl_sync(kFull, sub, src);
-                const double sv = __shfl_sync(kFull, s, src);
-                const double *vr = V + (size_t)sj * k;
+        // consume queued (code, s) pairs [0, n) in order
+        auto drain = [&](int n) {
+            __syncwarp();
+            int e = 0;
+            for (; e + U <= n; e += U) {
+                double vv[U][KPL];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const double *vr = V + (size_t)q_code[e + u] * k;
+#pragma unroll
+                    for (int q = 0; q < KPL; ++q) {
+                        const int j = lane + 32 * q;
+                        vv[u][q] = j < k ? __ldg(vr + j) : 0.0;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const double sv = q_val[e + u];
+#pragma unroll
+                    for (int q = 0; q < KPL; ++q) acc[q] = __dadd_rn(acc[q], __dmul_rn(sv, vv[u][q]));
+                }
+            }
+            for (; e < n; ++e) {
+                const double *vr = V + (size_t)q_code[e] * k;
+                const double sv = q_val[e];
 #pragma unroll
                 for (int q = 0; q < KPL; ++q) {
                     const int j = lane + 32 * q;
                     if (j < k) acc[q] = __dadd_rn(acc[q], __dmul_rn(sv, __ldg(vr + j)));
                 }
             }
+            __syncwarp();
+        };
+        double tsum = 0.0;
+        bool ok = true, ovf = false;
+        int nq = 0;
+        for_entries_by<8, false>(c, lo, hi, lookup, [&](int32_t m, float x) {
+            if (m >= 0 && norm) {
+                ok = ok && small_integer((double)x);
+                tsum += (double)x;
+            }
+            const bool hv = m >= 0 && m < d;
+            const unsigned mask = __ballot_sync(kFull, hv);
+            if (!mask) return;
+            if (nq + __popc(mask) > kProjQueue) {
+                ovf = true;
+                return;
+            }
+            if (hv) {
+                const int pos = nq + __popc(mask & ((1u << lane) - 1u));
+                q_code[pos] = m;
+                q_x[pos] = x;
+            }
+            nq += __popc(mask);
         });
+        double scale = 1.0;
+        if (norm) {
+            double total;
+            if (__all_sync(kFull, ok)) {
+                total = warp_sum(tsum);
+            } else {
+                OrderedSum ts;
+                for_entries_by<4, false>(c, lo, hi, lookup,
+                                         [&](int32_t m, float x) { ts.add(m >= 0 ? (double)x : 0.0); });
+                total = ts.acc;
+            }
+            scale = total > 0.0 ? c.target_sum / total : 1.0;
+        }
+        if (!ovf) {
+            __syncwarp();
+            for (int e = lane; e < nq; e += 32) q_val[e] = scale_value(t, q_code[e], transform_value(c, scale, q_x[e]));
+            drain(nq);
+        } else {  // second read, draining whenever the queue fills
+            nq = 0;
+            __syncwarp();
+            for_entries_by<8, true>(c, lo, hi, lookup, [&](int32_t m, float x) {
+                const bool hv = m >= 0 && m < d;
+                const unsigned mask = __ballot_sync(kFull, hv);
+                if (!mask) return;
+                if (nq + 32 > kProjQueue) {
+                    drain(nq);
+                    nq = 0;
+                }
+                if (hv) {
+                    const int pos = nq + __popc(mask & ((1u << lane) - 1u));
+                    q_code[pos] = m;
+                    q_val[pos] = scale_value(t, m, transform_value(c, scale, x));
+                }
+                nq += __popc(mask);
+            });
+            drain(nq);
+        }
         float *o = out + (size_t)(by_span ? i : row) * k;
 #pragma unroll
         for (int q = 0; q < KPL; ++q) {
@@ -162,20 +293,32 @@ int launch_gene_stats(const DevChunk &c, double *out, cudaStream_t st) {
     return CREST_OK;
 }
 
-int launch_project(const DevChunk &c, const int32_t *sub_map, const DevScale &t, const double *V, int k,
+template <int KPL>
+static int launch_project_k(const DevChunk &c, const int32_t *code, int64_t d, const DevScale &t, const double *V,
+                            int k, float *out, int by_span, cudaStream_t st) {
+    const int blocks = (int)std::min<int64_t>(ceil_div(c.n_spans, kProjWarps), device_sms());
+    if (codes_in_smem(c.n_gene_map, d, kProjSmemFixed)) {
+        const size_t smem = kProjSmemFixed + 2 * (size_t)round_up(c.n_gene_map, 8);
+        CREST_CUDA_TRY(cudaFuncSetAttribute(k_project<KPL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_project<KPL, true><<<blocks, kProjWarps * 32, smem, st>>>(c, code, (int32_t)d, t, V, k, out, by_span);
+    } else {
+        CREST_CUDA_TRY(cudaFuncSetAttribute(k_project<KPL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)kProjSmemFixed));
+        k_project<KPL, false><<<blocks, kProjWarps * 32, kProjSmemFixed, st>>>(c, code, (int32_t)d, t, V, k, out,
+                                                                                by_span);
+    }
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
+}
+
+int launch_project(const DevChunk &c, const int32_t *code, int64_t d, const DevScale &t, const double *V, int k,
                    float *out, int by_span, cudaStream_t st) {
     if (c.n_spans == 0 || k == 0) return CREST_OK;
     CREST_REQUIRE(k <= 128, CREST_EINVAL, "project supports k <= 128 (got %d)", k);
-    const int g = grid_for_spans(c.n_spans, device_sms());
     prof::Scope ps("project_csr", st);
-    if (k <= 32)
-        k_project<1><<<g, 256, 0, st>>>(c, sub_map, t, V, k, out, by_span);
-    else if (k <= 64)
-        k_project<2><<<g, 256, 0, st>>>(c, sub_map, t, V, k, out, by_span);
-    else
-        k_project<4><<<g, 256, 0, st>>>(c, sub_map, t, V, k, out, by_span);
-    CREST_CUDA_TRY(cudaGetLastError());
-    return CREST_OK;
+    if (k <= 32) return launch_project_k<1>(c, code, d, t, V, k, out, by_span, st);
+    if (k <= 64) return launch_project_k<2>(c, code, d, t, V, k, out, by_span, st);
+    return launch_project_k<4>(c, code, d, t, V, k, out, by_span, st);
 }
 
 // bias[g] = clip(-mean[g] / std[g]) (the scaled value of a zero entry).

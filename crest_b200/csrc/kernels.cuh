@@ -23,8 +23,16 @@ int launch_qc(const DevChunk &c, const uint8_t *flag, uint32_t *gene_ncells, dou
               const SpanOut *span, const RowOut *row, cudaStream_t st);
 int launch_gene_stats(const DevChunk &c, double *out, cudaStream_t st);
 // out row index: the cell's row, or the span index when by_span != 0
-int launch_project(const DevChunk &c, const int32_t *sub_map, const DevScale &t, const double *V, int k,
+// code: per-gene HVG codes from launch_hvg_code (d = number of HVG columns)
+int launch_project(const DevChunk &c, const int32_t *code, int64_t d, const DevScale &t, const double *V, int k,
                    float *out, int by_span, cudaStream_t st);
+// code[g] (g < c.n_gene_map): -1 dropped gene, sub_map[gene_map[g]] in [0, d)
+// for an HVG column, d for another kept gene.
+int launch_hvg_code(const DevChunk &c, const int32_t *sub_map, int64_t n_vars, int64_t d, int32_t *code,
+                    cudaStream_t st);
+// Largest dynamic shared memory a kernel here asks for (bytes).
+constexpr int kMaxSmem = 220 * 1024;
+bool codes_in_smem(int64_t n_gene_map, int64_t d, size_t other_smem);
 int launch_scale_bias(const double *mean, const double *std, double mv, int64_t d, double *bias, cudaStream_t st);
 
 // ------------------------------------------------------------------ Gram
@@ -49,7 +57,7 @@ struct GramWork {
 size_t gram_tile_bytes(int precision, int64_t d_pad, int64_t m_cap);
 // Densify spans [0, c.n_spans) of a chunk (n_spans <= m_cap) into the tile
 // and accumulate its colsum / kept count.
-int launch_densify(const DevChunk &c, const int32_t *sub_map, const DevScale &t, const GramWork &w,
+int launch_densify(const DevChunk &c, const int32_t *code, const DevScale &t, const GramWork &w,
                    cudaStream_t st);
 // gram (d x d row-major, upper triangle) += T T^T of the current tile; adds
 // colsum_chunk to colsum.

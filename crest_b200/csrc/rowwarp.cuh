@@ -3,11 +3,11 @@
 // One warp owns one cell (one span of the chunk).  Its entries are read in
 // segments of 32 consecutive entries (lane j holds entry s + j), several
 // segments per iteration so each warp keeps more loads in flight.  All
-// per-cell f64 sums are formed in the reference's entry order
-// (src/kernels.rs:69-76, 170-183): segments are folded lane by lane.  When
-// every value seen so far is an integer below 2^24 all partial sums are
-// exact, so a shuffle tree gives the identical result faster; the first
-// non-integer segment switches the cell to the sequential fold.
+// per-cell f64 sums equal the reference's entry-order sums
+// (src/kernels.rs:69-76, 170-183).  When every value of the cell is an
+// integer below 2^24 (raw counts) all partial sums are exact, so per-lane
+// partials and one shuffle tree give the identical result; otherwise the
+// segments are folded lane by lane in entry order.
 #pragma once
 
 #include "common.cuh"
@@ -52,11 +52,15 @@ struct OrderedSum {
     }
 };
 
-// Visit the entries of [lo, hi) in segment order; f(valid, mapped_gene, value)
-// is called by all 32 lanes once per segment (warp-collective operations
+// Visit the entries of [lo, hi) in segment order; f(mapped_gene, value) is
+// called by all 32 lanes once per segment (warp-collective operations
 // inside f are allowed).  Mapped gene is -1 for dropped or padding lanes.
-template <int U, class F>
-__device__ __forceinline__ void for_entries(const DevChunk &c, int64_t lo, int64_t hi, F &&f) {
+// LAST: the final read of these entries in the kernel (streaming loads);
+// earlier passes use cached loads so the next pass finds them in L2.
+// for_entries_by: the same visit with the gene code taken from lookup(g)
+// (g < n_gene_map guaranteed) instead of the chunk's gene_map.
+template <int U, bool LAST, class L, class F>
+__device__ __forceinline__ void for_entries_by(const DevChunk &c, int64_t lo, int64_t hi, L &&lookup, F &&f) {
     const int lane = lane_id();
     for (int64_t s = lo; s < hi; s += 32 * U) {
         uint32_t g[U];
@@ -65,26 +69,64 @@ __device__ __forceinline__ void for_entries(const DevChunk &c, int64_t lo, int64
         for (int u = 0; u < U; ++u) {
             const int64_t e = s + u * 32 + lane;
             const bool v = e < hi;
-            g[u] = v ? __ldcs(c.genes + e) : 0u;
-            x[u] = v ? __ldcs(c.values + e) : 0.0f;
+            g[u] = v ? (LAST ? __ldcs(c.genes + e) : __ldg(c.genes + e)) : 0u;
+            x[u] = v ? (LAST ? __ldcs(c.values + e) : __ldg(c.values + e)) : 0.0f;
         }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             if (s + u * 32 >= hi) break;  // warp-uniform
             const int64_t e = s + u * 32 + lane;
-            const int32_t m = e < hi ? map_gene(c, g[u]) : -1;
+            const int32_t m = (e < hi && (int64_t)g[u] < c.n_gene_map) ? lookup(g[u]) : -1;
             f(m, x[u]);
         }
     }
+}
+
+template <int U, bool LAST = true, class F>
+__device__ __forceinline__ void for_entries(const DevChunk &c, int64_t lo, int64_t hi, F &&f) {
+    for_entries_by<U, LAST>(c, lo, hi, [&](uint32_t g) { return (int32_t)__ldg(c.gene_map + g); }, f);
+}
+
+// Integer test of the fast paths: every partial sum of such values stays an
+// exactly representable integer, so any summation order gives the in-order
+// f64 result.
+__device__ __forceinline__ bool small_integer(double v) { return v == rint(v) && fabs(v) < 16777216.0; }
+
+// Warp sum of per-lane f64 partials (exact when they are integers).
+__device__ __forceinline__ double warp_sum(double s) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+    return s;
+}
+
+// Total of the kept-gene values of a cell when all of them are integers
+// below 2^24 (raw counts): lanes keep private partial sums, one reduction at
+// the end.  Returns false (and no total) when some value is not.
+__device__ __forceinline__ bool integral_total(const DevChunk &c, int64_t lo, int64_t hi, double &out) {
+    double s = 0.0;
+    bool ok = true;
+    for_entries<8, false>(c, lo, hi, [&](int32_t m, float x) {
+        if (m < 0) return;
+        const double v = (double)x;
+        ok = ok && small_integer(v);
+        s += v;
+    });
+    if (!__all_sync(kFull, ok)) return false;
+    out = warp_sum(s);
+    return true;
 }
 
 // Per-cell normalisation factor: target/total over kept genes, or 1
 // (src/kernels.rs:69-78).
 __device__ __forceinline__ double cell_scale(const DevChunk &c, int64_t lo, int64_t hi) {
     if (!(c.target_sum > 0.0)) return 1.0;
-    OrderedSum tot;
-    for_entries<4>(c, lo, hi, [&](int32_t m, float x) { tot.add(m >= 0 ? (double)x : 0.0); });
-    return tot.acc > 0.0 ? c.target_sum / tot.acc : 1.0;
+    double total;
+    if (!integral_total(c, lo, hi, total)) {
+        OrderedSum tot;
+        for_entries<4, false>(c, lo, hi, [&](int32_t m, float x) { tot.add(m >= 0 ? (double)x : 0.0); });
+        total = tot.acc;
+    }
+    return total > 0.0 ? c.target_sum / total : 1.0;
 }
 
 // The lazy transform of one value (src/kernels.rs:79-82).

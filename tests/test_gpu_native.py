@@ -10,6 +10,7 @@ import pytest
 
 import oracle
 from crest_b200 import _native
+from oracle import pipeline as op
 
 pytestmark = pytest.mark.gpu
 
@@ -224,6 +225,48 @@ def test_pca_from_gram_matches_lapack(d, k):
     assert np.all(cos > 1 - 1e-9), cos.min()
     imax = np.argmax(np.abs(L1), axis=0)
     assert np.all(L1[imax, np.arange(k)] > 0)
+
+
+def _gram_with_spectrum(lam, n, seed):
+    """(gram, colsum) whose covariance has eigenvalues lam and random eigenvectors."""
+    rng = np.random.default_rng(seed)
+    d = len(lam)
+    Q = np.linalg.qr(rng.standard_normal((d, d)))[0]
+    cov = (Q * lam) @ Q.T
+    cov = (cov + cov.T) / 2
+    c = rng.uniform(0, 50, d)
+    return (n - 1) * cov + np.outer(c, c) / n, c
+
+
+@pytest.mark.parametrize("kind", ["single_cell", "decay", "rank_deficient", "flat"])
+def test_pca_from_gram_spectra(kind):
+    """Spectra the block solver meets: one dominant component over a tight
+    cluster just above a dense bulk (scaled single-cell data), a power-law
+    decay, fewer cells than genes (exact zeros) and a nearly flat spectrum."""
+    rng = np.random.default_rng(7)
+    d, k, n = 1200, 50, 100_000
+    if kind == "single_cell":
+        lam = np.concatenate([[7.35], rng.uniform(1.0306, 1.0455, 49), 0.9 + 0.13 * rng.beta(2, 1.2, d - 50)])
+    elif kind == "decay":
+        lam = 100.0 * np.arange(1, d + 1) ** -1.5
+    elif kind == "rank_deficient":
+        n = 120
+        lam = np.concatenate([rng.exponential(1, n - 1) + 0.1, np.zeros(d - n + 1)])
+    else:
+        lam = 1 + 1e-3 * rng.standard_normal(d)
+    gram, colsum = _gram_with_spectrum(lam, n, 3)
+    v0, L0, t0 = oracle.pca_from_gram(gram, colsum, n, k)
+    v1, L1, t1 = _native.pca_from_gram(gram, colsum, n, k)
+    assert abs(t1 - t0) <= 1e-12 * abs(t0)
+    assert np.max(np.abs(v1 - v0)) <= 1e-10 * v0[0]
+    assert float(op.subspace_angles_deg(L0, L1).max()) <= 1e-5
+    # separated components: same direction and sign
+    gap = np.full(k, np.inf)
+    gap[:-1] = np.minimum(gap[:-1], (v0[:-1] - v0[1:]) / v0[0])
+    gap[1:] = np.minimum(gap[1:], (v0[:-1] - v0[1:]) / v0[0])
+    sep = gap[:-1] >= 1e-4
+    cos = (L0 * L1).sum(0)[:-1][sep]
+    assert np.all(cos > 1 - 1e-9), cos.min()
 
 
 def test_pca_from_gram_errors():
