@@ -59,6 +59,7 @@ _SIGS = {
     "crest_device_count": [],
     "crest_set_device": [C.c_int],
     "crest_qc": [P, P, I64, P, P, P, I64, P, P],
+    "crest_qc_static": [P, P, I64, P, P, P, I64, P, P],
     "crest_gene_stats": [P, I64, P],
     "crest_gram_accumulate": [P, P, I64, P, I64, P, P, I32],
     "crest_pca_from_gram": [P, P, I64, I64, I64, P, P, P, P],

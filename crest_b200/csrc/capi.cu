@@ -110,7 +110,7 @@ static int get_ctx(Ctx **out) {
 // ------------------------------------------------------- chunk validation
 // src/py.rs:162-189: lengths, exactly one of cells/indptr, sorted cells,
 // monotone indptr spanning the chunk.
-static int validate_chunk(const crest_chunk *c) {
+int validate_chunk(const crest_chunk *c) {
     CREST_REQUIRE(c != nullptr, CREST_EINVAL, "chunk is NULL");
     CREST_REQUIRE(c->nnz >= 0 && c->n_cell_map >= 0 && c->n_gene_map >= 0, CREST_EINVAL, "negative length");
     CREST_REQUIRE(c->nnz == 0 || (c->genes && c->values), CREST_EINVAL, "genes/values are NULL");
@@ -194,7 +194,7 @@ static int stage_chunk(Ctx &x, const crest_chunk *c, const HostSpans &s, DevChun
     return CREST_OK;
 }
 
-static int check_maps(const crest_chunk *c, int64_t n_vars) {
+int check_maps(const crest_chunk *c, int64_t n_vars) {
     int32_t mx = -1;
     for (int64_t i = 0; i < c->n_gene_map; ++i) mx = std::max(mx, c->gene_map[i]);
     CREST_REQUIRE((int64_t)mx + 1 <= n_vars, CREST_EINVAL, "gene_map holds var %d but n_vars is %lld", (int)mx,

@@ -72,6 +72,11 @@ inline DevChunk slice(const DevChunk &c, int64_t s0, int64_t n) {
     return r;
 }
 
+// Chunk checks of the reference's binding (src/py.rs:162-193): lengths, one
+// of cells / indptr, sorted cells, monotone indptr; gene_map values < n_vars.
+int validate_chunk(const crest_chunk *c);
+int check_maps(const crest_chunk *c, int64_t n_vars);
+
 // code: per-gene HVG codes from launch_hvg_code
 int gram_over_chunk(const DevChunk &dc, const int32_t *code, const DevScale &ds, GramWork &w, double *gram,
                     double *colsum, cudaStream_t st);

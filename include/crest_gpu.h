@@ -115,6 +115,20 @@ int crest_qc(const crest_chunk *chunk, const uint8_t *flag, int64_t n_vars, doub
              uint32_t *cell_ngenes, double *cell_flag, int64_t n_rows, uint32_t *gene_ncells,
              double *gene_total);
 
+/* crest_qc_static: no counterpart in the reference.  Same arguments and
+ * results as crest_qc, computed without allocating device memory: the
+ * kernel runs on a fixed scratch array compiled into the library (about
+ * 12 MB per device), for callers that must not have a library allocate (or
+ * free, with its implicit device synchronisation) device memory for them.
+ * Limits: CSR chunks (indptr) only, nnz <= 2^20, cells per chunk <= 2^16,
+ * n_gene_map and n_vars <= 2^16; larger chunks return CREST_EINVAL.  The
+ * first call on a device looks the scratch up (cudaGetSymbolAddress) and
+ * should precede any stream capture.  Calls are serialised process-wide
+ * (they share the scratch) and return after the results are on the host. */
+int crest_qc_static(const crest_chunk *chunk, const uint8_t *flag, int64_t n_vars, double *cell_total,
+                    uint32_t *cell_ngenes, double *cell_flag, int64_t n_rows, uint32_t *gene_ncells,
+                    double *gene_total);
+
 /* gene_stats: src/py.rs:221-232, src/kernels.rs:144-160.  out is
  * (n_vars, 5) row-major: [sum x, sum x^2, sum expm1 x, sum expm1(x)^2, nnz]. */
 int crest_gene_stats(const crest_chunk *chunk, int64_t n_vars, double *out);
