@@ -78,6 +78,24 @@ int device_sms() {
     return cache[dev];
 }
 
+int ensure_smem_attr(const void *kernel, size_t bytes) {
+    int dev = 0;
+    CREST_CUDA_TRY(cudaGetDevice(&dev));
+    static std::mutex mu;
+    static std::vector<std::pair<std::pair<const void *, int>, size_t>> done;
+    std::lock_guard<std::mutex> lock(mu);
+    for (auto &e : done)
+        if (e.first.first == kernel && e.first.second == dev && e.second >= bytes) return CREST_OK;
+    CREST_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    for (auto &e : done)
+        if (e.first.first == kernel && e.first.second == dev) {
+            e.second = bytes;
+            return CREST_OK;
+        }
+    done.push_back({{kernel, dev}, bytes});
+    return CREST_OK;
+}
+
 // ------------------------------------------------------------------ context
 // Per-device staging state of the per-chunk API.  The reference's native
 // functions are called sequentially from one Python thread; a mutex keeps
@@ -86,7 +104,7 @@ struct Ctx {
     std::mutex mu;
     bool ready = false;
     cudaStream_t st = nullptr;
-    DevBuf genes, values, span_ptr, span_cell, cell_map, gene_map, flag, sub_map, code;
+    DevBuf genes, values, span_ptr, span_cell, cell_map, gene_map, flag, sub_map, code, counter;
     DevBuf out0, out1, out2, out3, out4, out5;
     DevBuf mean, std_, bias, gram, colsum, vecs, vals, total, loadings;
     GramBufs gb;
@@ -229,7 +247,7 @@ static int check_sub_map(const int32_t *sub_map, int64_t n_vars, int64_t d) {
 
 int stage_hvg_code(const DevChunk &dc, const int32_t *sub_map, int64_t n_vars, int64_t d, DevBuf &buf,
                    cudaStream_t st) {
-    CREST_TRY(buf.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(dc.n_gene_map, 1)));
+    CREST_TRY(buf.ensure(std::max<size_t>(hvg_code_bytes(dc.n_gene_map), 16)));
     return launch_hvg_code(dc, sub_map, n_vars, d, buf.as<int32_t>(), st);
 }
 
@@ -452,8 +470,9 @@ int crest_project(const crest_chunk *chunk, const int32_t *sub_map, int64_t n_va
     CREST_TRY(upload(x->loadings, loadings, d * k, st));
     CREST_TRY(zeros<float>(x->out3, s.n * k, st));
     CREST_TRY(stage_hvg_code(dc, x->sub_map.as<int32_t>(), n_vars, d, x->code, st));
+    CREST_TRY(x->counter.ensure(sizeof(unsigned int)));
     CREST_TRY(launch_project(dc, x->code.as<int32_t>(), d, ds, x->loadings.as<double>(), (int)k,
-                             x->out3.as<float>(), 1, st));
+                             x->out3.as<float>(), 1, x->counter.as<unsigned int>(), st));
     std::vector<float> part(s.n * k);
     if (s.n * k)
         CREST_CUDA_TRY(cudaMemcpyAsync(part.data(), x->out3.ptr, 4 * s.n * k, cudaMemcpyDeviceToHost, st));

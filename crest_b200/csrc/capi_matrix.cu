@@ -27,7 +27,7 @@ struct crest_matrix {
     crest::DevBuf buf_idx[2], buf_val[2];
     cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
     // per-pass staging
-    crest::DevBuf cell_map, gene_map, flag, sub_map, code, mean, std_, bias;
+    crest::DevBuf cell_map, gene_map, flag, sub_map, code, counter, mean, std_, bias;
     crest::DevBuf out[5];
 };
 
@@ -461,8 +461,10 @@ int crest_pca_project(crest_pca *p, crest_matrix *m, const int64_t *cell_map, co
     CREST_CUDA_TRY(cudaGetLastError());
     const DevChunk proto = base_chunk(m, target_sum, log1p);
     CREST_TRY(stage_hvg_code(proto, m->sub_map.as<int32_t>(), n_vars, p->d, m->code, st));
+    CREST_TRY(m->counter.ensure(sizeof(unsigned int)));
     CREST_TRY(for_each_piece(m, proto, m->n_cells, [&](const DevChunk &c) {
-        return launch_project(c, m->code.as<int32_t>(), p->d, ds, p->vecs.as<double>(), (int)p->k, X, 0, st);
+        return launch_project(c, m->code.as<int32_t>(), p->d, ds, p->vecs.as<double>(), (int)p->k, X, 0,
+                              m->counter.as<unsigned int>(), st);
     }));
     if (out_mem != CREST_MEM_DEVICE && n_rows * p->k)
         CREST_CUDA_TRY(cudaMemcpyAsync(out, X, 4 * (size_t)(n_rows * p->k), cudaMemcpyDeviceToHost, st));

@@ -51,11 +51,12 @@ struct GramBufs {
         w.precision = precision;
         CREST_TRY(tile.ensure(gram_tile_bytes(precision, w.d_pad, m_cap)));
         CREST_TRY(colsum_chunk.ensure(sizeof(double) * (size_t)w.d_pad));
-        CREST_TRY(n_kept.ensure(sizeof(int64_t)));
+        CREST_TRY(n_kept.ensure(2 * sizeof(int64_t)));  // kept count, then the work counter
         CREST_TRY(shift.ensure(sizeof(double) * (size_t)w.d_pad));
         w.tile = tile.ptr;
         w.colsum_chunk = colsum_chunk.as<double>();
         w.n_kept = n_kept.as<int64_t>();
+        w.counter = reinterpret_cast<unsigned int *>(n_kept.as<int64_t>() + 1);
         w.part32 = nullptr;
         w.shift = shift.as<double>();
         return CREST_OK;

@@ -307,11 +307,11 @@ int jacobi(const double *A, int n_in, double *Vwork, double *V, double *vals, in
     prof::Scope ps("eig_jacobi", st);
     if (n <= kJacobiSmemV) {
         const size_t smem = sizeof(double) * ((size_t)n * (n + 1) + (size_t)n * n);
-        CREST_CUDA_TRY(cudaFuncSetAttribute(k_jacobi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CREST_TRY(ensure_smem_attr((const void *)k_jacobi<true>, (size_t)smem));
         k_jacobi<true><<<1, 1024, smem, st>>>(A, n_in, n, nullptr, V, vals, 40, sweeps);
     } else {
         const size_t smem = sizeof(double) * (size_t)n * (size_t)(n + 1);
-        CREST_CUDA_TRY(cudaFuncSetAttribute(k_jacobi<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CREST_TRY(ensure_smem_attr((const void *)k_jacobi<false>, (size_t)smem));
         k_jacobi<false><<<1, 1024, smem, st>>>(A, n_in, n, Vwork, V, vals, 40, sweeps);
     }
     CREST_CUDA_TRY(cudaGetLastError());
@@ -645,7 +645,7 @@ int orthonormalise(EigWork &w, double *Y, int64_t d, int j0, int q, bool shifted
     double *Rinv = w.Q.as<double>();
     int *fail = w.fail.as<int>();
     const size_t csmem = sizeof(double) * 2 * (size_t)q * q;
-    CREST_CUDA_TRY(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmem));
+    CREST_TRY(ensure_smem_attr((const void *)k_chol_inv, (size_t)csmem));
     const int passes = shifted ? 3 : 2;
     for (int pass = 0; pass < passes; ++pass) {
         if (j0 > 0) {  // remove the locked directions (twice for orthogonality)

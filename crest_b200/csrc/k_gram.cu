@@ -18,6 +18,8 @@
 //    contracted on the tcgen05 tensor cores (k_gram_tc.cu), same FP64 fold.
 #include <cuda_bf16.h>
 
+#include <type_traits>
+
 #include "kernels.cuh"
 #include "prof.cuh"
 #include "rowwarp.cuh"
@@ -54,22 +56,31 @@ __global__ void k_tile_shift(int precision, const double *__restrict__ bias, int
 // code[g] for a store gene id g < n_gene_map: -1 when the gene is dropped,
 // sub_map[gene_map[g]] in [0, d) for an HVG column, d for another kept gene
 // (it still counts towards the cell total).  One table lookup per entry
-// then serves both the normalisation total and the HVG selection.
+// then serves both the normalisation total and the HVG selection.  The
+// same codes follow as int16 (when d < 2^15 - 1), zero-padded to a multiple
+// of 8, for the kernels that copy the table to shared memory.
 __global__ void k_hvg_code(const int32_t *__restrict__ gene_map, int64_t n_gene_map,
                            const int32_t *__restrict__ sub_map, int64_t n_vars, int64_t d, int32_t *__restrict__ code) {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= n_gene_map) return;
-    const int32_t m = gene_map[g];
+    if (g >= round_up(n_gene_map, 8)) return;
     int32_t v = -1;
-    if (m >= 0) v = (m < n_vars && sub_map[m] >= 0) ? sub_map[m] : (int32_t)d;
-    code[g] = v;
+    if (g < n_gene_map) {
+        const int32_t m = gene_map[g];
+        if (m >= 0) v = (m < n_vars && sub_map[m] >= 0) ? sub_map[m] : (int32_t)d;
+        code[g] = v;
+    }
+    if (d < 32767) const_cast<int16_t *>(codes16(code, n_gene_map))[g] = (int16_t)v;
+}
+
+size_t hvg_code_bytes(int64_t n_gene_map) {
+    return 4 * (size_t)round_up(n_gene_map, 4) + 2 * (size_t)round_up(n_gene_map, 8);
 }
 
 int launch_hvg_code(const DevChunk &c, const int32_t *sub_map, int64_t n_vars, int64_t d, int32_t *code,
                     cudaStream_t st) {
     if (c.n_gene_map <= 0) return CREST_OK;
-    k_hvg_code<<<(unsigned)ceil_div(c.n_gene_map, 256), 256, 0, st>>>(c.gene_map, c.n_gene_map, sub_map, n_vars, d,
-                                                                      code);
+    k_hvg_code<<<(unsigned)ceil_div(round_up(c.n_gene_map, 8), 256), 256, 0, st>>>(c.gene_map, c.n_gene_map, sub_map,
+                                                                                   n_vars, d, code);
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
 }
@@ -82,17 +93,20 @@ bool codes_in_smem(int64_t n_gene_map, int64_t d, size_t other_smem) {
 
 // ------------------------------------------------------------- densify
 // Warp per cell row i of the tile (i < m_pad, padding rows included),
-// written straight into the (L2-resident) tile.  One read of the cell's
-// entries: lanes add up the kept values (the normalisation total) and queue
-// the HVG entries (code, raw value), in entry order, in a per-warp
-// shared-memory queue.  Then the row is filled with the zero-entry value of
-// every gene -- the shift for kept cells, 0 for dropped / padding rows --
-// with 16-byte stores and, after a warp barrier that orders the two sets of
-// stores, the queued entries are transformed and stored.  A cell with more
-// than kQueue HVG entries, or whose total needs the in-order fold, reads its
-// entries a second time.  The colsum of S (FP32 / BF16X3) is privatised per
-// block in shared memory.  Duplicate (cell, gene) entries are not supported
-// (one of them lands in the tile).
+// written straight into the (L2-resident) tile.  Rows are handed out one at
+// a time through a counter, since cells differ in length.  One read of the
+// cell's entries (four per lane, 16-byte loads): lanes add up the kept
+// values (the normalisation total) and queue the HVG entries (code, raw
+// value), in entry order, in a per-warp shared-memory queue.  Then the row
+// is filled with the zero-entry value of every gene -- the shift for kept
+// cells, 0 for dropped / padding rows -- with 16-byte stores and, after a
+// warp barrier that orders the two sets of stores, the queued entries are
+// transformed and stored.  A cell with more than kQueue HVG entries, or
+// whose total needs the in-order fold, reads its entries a second time
+// (rare: such cells are the longest of a tile and would otherwise set its
+// duration).  The colsum of S (FP32 / BF16X3) is privatised per block in
+// shared memory.  Duplicate (cell, gene) entries are not supported (one of
+// them lands in the tile).
 template <int MODE>  // 0 FP64 (T = S), 1 FP32 (T = S + shift), 2 BF16X3 (hi/lo of S + shift)
 struct RowElem;
 template <> struct RowElem<0> { using T = double; };
@@ -100,7 +114,7 @@ template <> struct RowElem<1> { using T = float; };
 template <> struct RowElem<2> { using T = __nv_bfloat16; };
 
 constexpr int kDensifyWarps = 32;
-constexpr int kQueue = 256;
+constexpr int kQueue = 512;
 
 // bf16 split of a tile value (hi + lo ~ z to 2^-17 relative).  hi may come
 // from a double rounding through f32: any nearby bf16 works, lo holds the rest.
@@ -109,11 +123,13 @@ __device__ __forceinline__ void split_bf16(double z, __nv_bfloat16 &hi, __nv_bfl
     lo = __float2bfloat16_rn(__double2float_rn(z - (double)__bfloat162float(hi)));
 }
 
-template <int MODE>
+// Queued codes are int16 when the code table itself is (SMAP), else int32.
+template <int MODE, bool SMAP>
 static size_t densify_smem_fixed(int64_t d, int64_t d_pad) {
     using E = typename RowElem<MODE>::T;
+    using Q = typename std::conditional<SMAP, int16_t, int32_t>::type;
     const size_t priv = MODE != 0 ? sizeof(double) * (size_t)round_up(d, 2) + sizeof(E) * (size_t)d_pad : 0;
-    return priv + (size_t)kDensifyWarps * kQueue * (sizeof(int32_t) + sizeof(float));
+    return priv + (size_t)kDensifyWarps * kQueue * (sizeof(Q) + sizeof(float));
 }
 
 template <int MODE, bool SMAP>
@@ -121,38 +137,39 @@ __global__ void __launch_bounds__(kDensifyWarps * 32, 1) k_densify(DevChunk c, c
                                                                    DevScale t, const double *__restrict__ shift,
                                                                    int64_t d, int64_t d_pad, int64_t m_pad,
                                                                    void *tile, double *__restrict__ colsum,
-                                                                   int64_t *n_kept) {
+                                                                   int64_t *n_kept, unsigned int *counter) {
     using E = typename RowElem<MODE>::T;
+    using Q = typename std::conditional<SMAP, int16_t, int32_t>::type;
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     constexpr bool priv = MODE != 0;
     // [colsum of S (f64)] [shift row (tile type)]   (MODE != 0)
-    // [queue codes (int32)] [queue values (f32)] [codes (int16), SMAP]
+    // [queue values (f32)] [queue codes (Q)] [codes (int16), SMAP]
     double *s_col = reinterpret_cast<double *>(smem);
     E *shift_row = reinterpret_cast<E *>(smem + (priv ? sizeof(double) * (size_t)round_up(d, 2) : 0));
     unsigned char *qbase = reinterpret_cast<unsigned char *>(shift_row) + (priv ? sizeof(E) * (size_t)d_pad : 0);
-    int32_t *q_code = reinterpret_cast<int32_t *>(qbase) + (size_t)wid * kQueue;
-    float *q_x = reinterpret_cast<float *>(qbase + sizeof(int32_t) * (size_t)kDensifyWarps * kQueue) +
-                 (size_t)wid * kQueue;
-    int16_t *s_code = reinterpret_cast<int16_t *>(qbase + (sizeof(int32_t) + sizeof(float)) * (size_t)kDensifyWarps * kQueue);
+    float *q_x = reinterpret_cast<float *>(qbase) + (size_t)wid * kQueue;
+    Q *q_code = reinterpret_cast<Q *>(qbase + sizeof(float) * (size_t)kDensifyWarps * kQueue) + (size_t)wid * kQueue;
+    int16_t *s_code = reinterpret_cast<int16_t *>(qbase + (sizeof(Q) + sizeof(float)) * (size_t)kDensifyWarps * kQueue);
     if (priv) {
         for (int64_t j = threadIdx.x; j < d_pad; j += blockDim.x) shift_row[j] = (E)((shift && j < d) ? shift[j] : 0.0);
         for (int64_t j = threadIdx.x; j < d; j += blockDim.x) s_col[j] = 0.0;
     }
-    if (SMAP)
-        for (int64_t j = threadIdx.x; j < c.n_gene_map; j += blockDim.x) s_code[j] = (int16_t)code[j];
+    if (SMAP) copy_codes16(code, c.n_gene_map, s_code);
     __syncthreads();
     auto lookup = [&](uint32_t g) -> int32_t { return SMAP ? (int32_t)s_code[g] : __ldg(code + g); };
     const int32_t dd = (int32_t)d;
-    const int64_t warp = (int64_t)blockIdx.x * kDensifyWarps + wid;
-    const int64_t n_warps = (int64_t)gridDim.x * kDensifyWarps;
     const int64_t nvec = d_pad * (int64_t)sizeof(E) / 16;
     E *hi_plane = reinterpret_cast<E *>(tile);
     E *lo_plane = hi_plane + (size_t)m_pad * d_pad;  // BF16X3 only
     const uint4 zero = make_uint4(0, 0, 0, 0);
     const bool norm = c.target_sum > 0.0;
     int kept_count = 0;
-    for (int64_t i = warp; i < m_pad; i += n_warps) {
+    for (;;) {
+        int64_t i = 0;
+        if (lane == 0) i = atomicAdd(counter, 1u);
+        i = __shfl_sync(kFull, i, 0);
+        if (i >= m_pad) break;
         int64_t lo = 0, hi = 0, r = -1;
         if (i < c.n_spans) r = span_row(c, i, lo, hi);
         const bool kept = r >= 0;
@@ -161,24 +178,31 @@ __global__ void __launch_bounds__(kDensifyWarps * 32, 1) k_densify(DevChunk c, c
         bool ok = true, ovf = false;
         int nq = 0;
         if (kept) {
-            for_entries_by<8, false>(c, lo, hi, lookup, [&](int32_t m, float x) {
-                if (m >= 0 && norm) {
-                    ok = ok && small_integer((double)x);
-                    tsum += (double)x;
+            for_entries_x4<true>(c, lo, hi, lookup, [&](const int32_t (&m)[4], const float (&x)[4]) {
+                bool hv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (m[u] >= 0 && norm) {
+                        ok = ok && x[u] == rintf(x[u]) && fabsf(x[u]) < 16777216.0f;
+                        tsum += (double)x[u];
+                    }
+                    hv[u] = m[u] >= 0 && m[u] < dd;
                 }
-                const bool hv = m >= 0 && m < dd;
-                const unsigned mask = __ballot_sync(kFull, hv);
-                if (!mask) return;
-                if (nq + __popc(mask) > kQueue) {
+                int cnt;
+                int pos = nq + block_rank4(hv, cnt);
+                if (cnt == 0) return;
+                if (nq + cnt > kQueue) {
                     ovf = true;
                     return;
                 }
-                if (hv) {
-                    const int pos = nq + __popc(mask & ((1u << lane) - 1u));
-                    q_code[pos] = m;
-                    q_x[pos] = x;
-                }
-                nq += __popc(mask);
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (hv[u]) {
+                        q_code[pos] = (Q)m[u];
+                        q_x[pos] = x[u];
+                        ++pos;
+                    }
+                nq += cnt;
             });
         }
         // fill the row with the zero-entry values
@@ -227,7 +251,7 @@ __global__ void __launch_bounds__(kDensifyWarps * 32, 1) k_densify(DevChunk c, c
             }
         };
         if (!ovf) {
-            for (int e = lane; e < nq; e += 32) put(q_code[e], q_x[e]);
+            for (int e = lane; e < nq; e += 32) put((int32_t)q_code[e], q_x[e]);
         } else {
             for_entries_by<8, true>(c, lo, hi, lookup, [&](int32_t m, float x) {
                 if (m >= 0 && m < dd) put(m, x);
@@ -246,12 +270,13 @@ __global__ void __launch_bounds__(kDensifyWarps * 32, 1) k_densify(DevChunk c, c
 template <int MODE, bool SMAP>
 static int launch_densify_k(const DevChunk &c, const int32_t *code, const DevScale &t, const double *shift,
                             const GramWork &w, int64_t m_pad, size_t smem, cudaStream_t st) {
-    CREST_CUDA_TRY(cudaFuncSetAttribute(k_densify<MODE, SMAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CREST_TRY(ensure_smem_attr((const void *)k_densify<MODE, SMAP>, smem));
     int64_t blocks = ceil_div(m_pad, kDensifyWarps);
     const int64_t cap = (int64_t)device_sms();
     if (blocks > cap) blocks = cap;
     k_densify<MODE, SMAP><<<(unsigned)blocks, kDensifyWarps * 32, smem, st>>>(c, code, t, shift, w.d, w.d_pad, m_pad,
-                                                                               w.tile, w.colsum_chunk, w.n_kept);
+                                                                               w.tile, w.colsum_chunk, w.n_kept,
+                                                                               w.counter);
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
 }
@@ -259,12 +284,13 @@ static int launch_densify_k(const DevChunk &c, const int32_t *code, const DevSca
 template <int MODE>
 static int launch_densify_t(const DevChunk &c, const int32_t *code, const DevScale &t, const double *shift,
                             const GramWork &w, int64_t m_pad, cudaStream_t st) {
-    const size_t fixed = densify_smem_fixed<MODE>(w.d, w.d_pad);
+    const size_t fixed16 = densify_smem_fixed<MODE, true>(w.d, w.d_pad);
+    if (codes_in_smem(c.n_gene_map, w.d, fixed16))
+        return launch_densify_k<MODE, true>(c, code, t, shift, w, m_pad,
+                                            fixed16 + 2 * (size_t)round_up(c.n_gene_map, 8), st);
+    const size_t fixed = densify_smem_fixed<MODE, false>(w.d, w.d_pad);
     CREST_REQUIRE(fixed <= (size_t)kMaxSmem, CREST_EINVAL, "d=%lld too large for the densify shared buffers",
                   (long long)w.d);
-    if (codes_in_smem(c.n_gene_map, w.d, fixed))
-        return launch_densify_k<MODE, true>(c, code, t, shift, w, m_pad,
-                                            fixed + 2 * (size_t)round_up(c.n_gene_map, 8), st);
     return launch_densify_k<MODE, false>(c, code, t, shift, w, m_pad, fixed, st);
 }
 
@@ -273,7 +299,7 @@ int launch_densify(const DevChunk &c, const int32_t *code, const DevScale &t, co
     CREST_REQUIRE(c.n_spans <= w.m_cap, CREST_EINVAL, "tile holds %lld cells, chunk has %lld",
                   (long long)w.m_cap, (long long)c.n_spans);
     const int64_t m_pad = round_up(c.n_spans > 0 ? c.n_spans : 1, 64);
-    CREST_CUDA_TRY(cudaMemsetAsync(w.n_kept, 0, sizeof(int64_t), st));
+    CREST_CUDA_TRY(cudaMemsetAsync(w.n_kept, 0, 2 * sizeof(int64_t), st));  // kept count + work counter
     CREST_CUDA_TRY(cudaMemsetAsync(w.colsum_chunk, 0, sizeof(double) * (size_t)(w.d > 0 ? w.d : 1), st));
     const double *shift = nullptr;
     if (w.precision != CREST_GRAM_FP64 && t.scale) {
@@ -490,8 +516,7 @@ int launch_syrk_fold(const GramWork &w, int64_t m, const DevScale &t, double *gr
         const int64_t nb = w.d_pad / kBM;
         const int64_t tiles = nb * (nb + 1) / 2;
         prof::Scope ps("syrk_fp32", st);
-        CREST_CUDA_TRY(
-            cudaFuncSetAttribute(k_syrk_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSyrkF32Smem));
+        CREST_TRY(ensure_smem_attr((const void *)k_syrk_f32, (size_t)kSyrkF32Smem));
         k_syrk_f32<<<(unsigned)tiles, 256, kSyrkF32Smem, st>>>((const float *)w.tile, w.d, w.d_pad, m_pad, nb, shift,
                                                               w.colsum_chunk, w.n_kept, gram);
         CREST_CUDA_TRY(cudaGetLastError());

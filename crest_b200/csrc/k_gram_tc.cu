@@ -453,7 +453,7 @@ int syrk_bf16x3_fold(const GramWork &w, int64_t m_pad, const DevScale &t, double
     a.G = gram;
     a.err = err;
     const size_t smem = 1024 + (size_t)kStages * kStageBytes;
-    CREST_CUDA_TRY(cudaFuncSetAttribute(k_syrk_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CREST_TRY(ensure_smem_attr((const void *)k_syrk_bf16x3, (size_t)smem));
     const int tiles = a.nb * (a.nb + 1) / 2;
     prof::Scope ps("syrk_bf16x3_tcgen05", st);
     k_syrk_bf16x3<<<tiles, kThreads, smem, st>>>(map, a);

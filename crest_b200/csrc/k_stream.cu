@@ -5,6 +5,8 @@
 // entry (4 B gene id + 4 B value) is read once from HBM with streaming
 // loads, per-cell sums are formed in the reference's entry order
 // (rowwarp.cuh), per-gene sums go to L2-resident accumulators.
+#include <type_traits>
+
 #include "kernels.cuh"
 #include "prof.cuh"
 #include "rowwarp.cuh"
@@ -125,53 +127,65 @@ __global__ void __launch_bounds__(256) k_gene_stats(DevChunk c, double *__restri
 // src/kernels.rs:352-371.  For each kept cell: a[j] = sum over HVG entries
 // (entry order) of s * V[sub, j] in f64 without fusing; out[row, j] += (f32)a[j].
 // Lane l owns components l, l+32, ... (k <= 128).  One read of the cell's
-// entries forms the normalisation total and queues the HVG entries (code,
-// raw value) in entry order in a per-warp shared-memory queue; once the
-// scale is known the queued values are transformed in parallel, and the
-// queue is consumed U entries at a time with all V-row loads issued before
-// the U ordered additions, so the L2 latency of the V gathers overlaps.  A
-// cell with more than kProjQueue HVG entries (or whose total needs the
-// in-order fold) reads its entries again.
+// entries (four per lane, 16-byte loads) forms the normalisation total and
+// queues the HVG entries (code, raw value) in entry order in a per-warp
+// shared-memory queue.  Once the scale is known the queue is consumed in
+// rounds of kProjStage entries: the lanes transform a round in parallel
+// into a staging buffer, then the round is added U entries at a time with
+// all V-row loads issued before the U ordered additions, so the L2 latency
+// of the V gathers overlaps.  A cell with more than kProjQueue HVG entries
+// (or whose total needs the in-order fold) reads its entries again.  Cells
+// are handed out one at a time through a counter.
 constexpr int kProjWarps = 32;
-constexpr int kProjQueue = 256;
-constexpr size_t kProjSmemFixed = (size_t)kProjWarps * kProjQueue * (sizeof(int32_t) + sizeof(float) + sizeof(double));
+constexpr int kProjQueue = 512;
+constexpr int kProjStage = 128;
+
+template <bool SMAP>
+constexpr size_t proj_smem_fixed() {
+    return (size_t)kProjWarps * (kProjQueue * ((SMAP ? sizeof(int16_t) : sizeof(int32_t)) + sizeof(float)) +
+                                 kProjStage * sizeof(double));
+}
 
 template <int KPL, bool SMAP>
 __global__ void __launch_bounds__(kProjWarps * 32, 1) k_project(DevChunk c, const int32_t *__restrict__ code,
                                                                 int32_t d, DevScale t, const double *__restrict__ V,
-                                                                int k, float *__restrict__ out, int by_span) {
-    constexpr int U = KPL >= 4 ? 4 : 8;
+                                                                int k, float *__restrict__ out, int by_span,
+                                                                unsigned int *counter) {
+    constexpr int U = KPL >= 2 ? 4 : 8;
+    using Q = typename std::conditional<SMAP, int16_t, int32_t>::type;
     extern __shared__ __align__(16) unsigned char smem[];
     const int wid = threadIdx.x >> 5, lane = lane_id();
-    double *q_val = reinterpret_cast<double *>(smem) + (size_t)wid * kProjQueue;
-    int32_t *q_code = reinterpret_cast<int32_t *>(smem + sizeof(double) * kProjWarps * kProjQueue) +
-                      (size_t)wid * kProjQueue;
-    float *q_x = reinterpret_cast<float *>(smem + (sizeof(double) + sizeof(int32_t)) * kProjWarps * kProjQueue) +
-                 (size_t)wid * kProjQueue;
-    int16_t *s_code = reinterpret_cast<int16_t *>(smem + kProjSmemFixed);
-    if (SMAP)
-        for (int64_t j = threadIdx.x; j < c.n_gene_map; j += blockDim.x) s_code[j] = (int16_t)code[j];
+    // [staged values (f64)] [queued raw values (f32)] [queued codes (Q)] [codes (int16), SMAP]
+    double *q_val = reinterpret_cast<double *>(smem) + (size_t)wid * kProjStage;
+    unsigned char *p1 = smem + sizeof(double) * kProjWarps * kProjStage;
+    float *q_x = reinterpret_cast<float *>(p1) + (size_t)wid * kProjQueue;
+    unsigned char *p2 = p1 + sizeof(float) * kProjWarps * kProjQueue;
+    Q *q_code = reinterpret_cast<Q *>(p2) + (size_t)wid * kProjQueue;
+    int16_t *s_code = reinterpret_cast<int16_t *>(smem + proj_smem_fixed<SMAP>());
+    if (SMAP) copy_codes16(code, c.n_gene_map, s_code);
     __syncthreads();
     auto lookup = [&](uint32_t g) -> int32_t { return SMAP ? (int32_t)s_code[g] : __ldg(code + g); };
-    const int64_t warp = (int64_t)blockIdx.x * kProjWarps + wid;
-    const int64_t n_warps = (int64_t)gridDim.x * kProjWarps;
     const bool norm = c.target_sum > 0.0;
-    for (int64_t i = warp; i < c.n_spans; i += n_warps) {
+    for (;;) {
+        int64_t i = 0;
+        if (lane == 0) i = atomicAdd(counter, 1u);
+        i = __shfl_sync(kFull, i, 0);
+        if (i >= c.n_spans) break;
         int64_t lo, hi;
         const int64_t row = span_row(c, i, lo, hi);
         if (row < 0) continue;
         double acc[KPL];
 #pragma unroll
         for (int q = 0; q < KPL; ++q) acc[q] = 0.0;
-        // consume queued (code, s) pairs [0, n) in order
-        auto drain = [&](int n) {
+        // add staged pairs (code q_code[base + e], value q_val[e]), e < n, in order
+        auto drain = [&](int base, int n) {
             __syncwarp();
             int e = 0;
             for (; e + U <= n; e += U) {
                 double vv[U][KPL];
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
-                    const double *vr = V + (size_t)q_code[e + u] * k;
+                    const double *vr = V + (size_t)q_code[base + e + u] * k;
 #pragma unroll
                     for (int q = 0; q < KPL; ++q) {
                         const int j = lane + 32 * q;
@@ -186,7 +200,7 @@ __global__ void __launch_bounds__(kProjWarps * 32, 1) k_project(DevChunk c, cons
                 }
             }
             for (; e < n; ++e) {
-                const double *vr = V + (size_t)q_code[e] * k;
+                const double *vr = V + (size_t)q_code[base + e] * k;
                 const double sv = q_val[e];
 #pragma unroll
                 for (int q = 0; q < KPL; ++q) {
@@ -199,24 +213,31 @@ __global__ void __launch_bounds__(kProjWarps * 32, 1) k_project(DevChunk c, cons
         double tsum = 0.0;
         bool ok = true, ovf = false;
         int nq = 0;
-        for_entries_by<8, false>(c, lo, hi, lookup, [&](int32_t m, float x) {
-            if (m >= 0 && norm) {
-                ok = ok && small_integer((double)x);
-                tsum += (double)x;
+        for_entries_x4<true>(c, lo, hi, lookup, [&](const int32_t (&m)[4], const float (&x)[4]) {
+            bool hv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (m[u] >= 0 && norm) {
+                    ok = ok && x[u] == rintf(x[u]) && fabsf(x[u]) < 16777216.0f;
+                    tsum += (double)x[u];
+                }
+                hv[u] = m[u] >= 0 && m[u] < d;
             }
-            const bool hv = m >= 0 && m < d;
-            const unsigned mask = __ballot_sync(kFull, hv);
-            if (!mask) return;
-            if (nq + __popc(mask) > kProjQueue) {
+            int cnt;
+            int pos = nq + block_rank4(hv, cnt);
+            if (cnt == 0) return;
+            if (nq + cnt > kProjQueue) {
                 ovf = true;
                 return;
             }
-            if (hv) {
-                const int pos = nq + __popc(mask & ((1u << lane) - 1u));
-                q_code[pos] = m;
-                q_x[pos] = x;
-            }
-            nq += __popc(mask);
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (hv[u]) {
+                    q_code[pos] = (Q)m[u];
+                    q_x[pos] = x[u];
+                    ++pos;
+                }
+            nq += cnt;
         });
         double scale = 1.0;
         if (norm) {
@@ -232,28 +253,32 @@ __global__ void __launch_bounds__(kProjWarps * 32, 1) k_project(DevChunk c, cons
             scale = total > 0.0 ? c.target_sum / total : 1.0;
         }
         if (!ovf) {
-            __syncwarp();
-            for (int e = lane; e < nq; e += 32) q_val[e] = scale_value(t, q_code[e], transform_value(c, scale, q_x[e]));
-            drain(nq);
-        } else {  // second read, draining whenever the queue fills
-            nq = 0;
+            for (int r0 = 0; r0 < nq; r0 += kProjStage) {
+                const int n = nq - r0 < kProjStage ? nq - r0 : kProjStage;
+                __syncwarp();
+                for (int e = lane; e < n; e += 32)
+                    q_val[e] = scale_value(t, q_code[r0 + e], transform_value(c, scale, q_x[r0 + e]));
+                drain(r0, n);
+            }
+        } else {  // second read, draining whenever the staging buffer fills
+            int ns = 0;
             __syncwarp();
             for_entries_by<8, true>(c, lo, hi, lookup, [&](int32_t m, float x) {
                 const bool hv = m >= 0 && m < d;
                 const unsigned mask = __ballot_sync(kFull, hv);
                 if (!mask) return;
-                if (nq + 32 > kProjQueue) {
-                    drain(nq);
-                    nq = 0;
+                if (ns + 32 > kProjStage) {
+                    drain(0, ns);
+                    ns = 0;
                 }
                 if (hv) {
-                    const int pos = nq + __popc(mask & ((1u << lane) - 1u));
-                    q_code[pos] = m;
+                    const int pos = ns + __popc(mask & ((1u << lane) - 1u));
+                    q_code[pos] = (Q)m;
                     q_val[pos] = scale_value(t, m, transform_value(c, scale, x));
                 }
-                nq += __popc(mask);
+                ns += __popc(mask);
             });
-            drain(nq);
+            drain(0, ns);
         }
         float *o = out + (size_t)(by_span ? i : row) * k;
 #pragma unroll
@@ -295,30 +320,32 @@ int launch_gene_stats(const DevChunk &c, double *out, cudaStream_t st) {
 
 template <int KPL>
 static int launch_project_k(const DevChunk &c, const int32_t *code, int64_t d, const DevScale &t, const double *V,
-                            int k, float *out, int by_span, cudaStream_t st) {
+                            int k, float *out, int by_span, unsigned int *counter, cudaStream_t st) {
+    CREST_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int), st));
     const int blocks = (int)std::min<int64_t>(ceil_div(c.n_spans, kProjWarps), device_sms());
-    if (codes_in_smem(c.n_gene_map, d, kProjSmemFixed)) {
-        const size_t smem = kProjSmemFixed + 2 * (size_t)round_up(c.n_gene_map, 8);
-        CREST_CUDA_TRY(cudaFuncSetAttribute(k_project<KPL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_project<KPL, true><<<blocks, kProjWarps * 32, smem, st>>>(c, code, (int32_t)d, t, V, k, out, by_span);
+    if (codes_in_smem(c.n_gene_map, d, proj_smem_fixed<true>())) {
+        const size_t smem = proj_smem_fixed<true>() + 2 * (size_t)round_up(c.n_gene_map, 8);
+        CREST_TRY(ensure_smem_attr((const void *)k_project<KPL, true>, smem));
+        k_project<KPL, true><<<blocks, kProjWarps * 32, smem, st>>>(c, code, (int32_t)d, t, V, k, out, by_span,
+                                                                     counter);
     } else {
-        CREST_CUDA_TRY(cudaFuncSetAttribute(k_project<KPL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)kProjSmemFixed));
-        k_project<KPL, false><<<blocks, kProjWarps * 32, kProjSmemFixed, st>>>(c, code, (int32_t)d, t, V, k, out,
-                                                                                by_span);
+        const size_t smem = proj_smem_fixed<false>();
+        CREST_TRY(ensure_smem_attr((const void *)k_project<KPL, false>, smem));
+        k_project<KPL, false><<<blocks, kProjWarps * 32, smem, st>>>(c, code, (int32_t)d, t, V, k, out, by_span,
+                                                                      counter);
     }
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
 }
 
 int launch_project(const DevChunk &c, const int32_t *code, int64_t d, const DevScale &t, const double *V, int k,
-                   float *out, int by_span, cudaStream_t st) {
+                   float *out, int by_span, unsigned int *counter, cudaStream_t st) {
     if (c.n_spans == 0 || k == 0) return CREST_OK;
     CREST_REQUIRE(k <= 128, CREST_EINVAL, "project supports k <= 128 (got %d)", k);
     prof::Scope ps("project_csr", st);
-    if (k <= 32) return launch_project_k<1>(c, code, d, t, V, k, out, by_span, st);
-    if (k <= 64) return launch_project_k<2>(c, code, d, t, V, k, out, by_span, st);
-    return launch_project_k<4>(c, code, d, t, V, k, out, by_span, st);
+    if (k <= 32) return launch_project_k<1>(c, code, d, t, V, k, out, by_span, counter, st);
+    if (k <= 64) return launch_project_k<2>(c, code, d, t, V, k, out, by_span, counter, st);
+    return launch_project_k<4>(c, code, d, t, V, k, out, by_span, counter, st);
 }
 
 // bias[g] = clip(-mean[g] / std[g]) (the scaled value of a zero entry).

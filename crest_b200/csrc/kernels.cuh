@@ -6,6 +6,9 @@
 namespace crest {
 
 int device_sms();  // SM count of the current device (cached per device)
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) once per kernel, device
+// and size instead of before every launch.
+int ensure_smem_attr(const void *kernel, size_t bytes);
 
 struct SpanOut {  // per-span QC results (per-chunk API)
     int64_t *row;
@@ -24,14 +27,28 @@ int launch_qc(const DevChunk &c, const uint8_t *flag, uint32_t *gene_ncells, dou
 int launch_gene_stats(const DevChunk &c, double *out, cudaStream_t st);
 // out row index: the cell's row, or the span index when by_span != 0
 // code: per-gene HVG codes from launch_hvg_code (d = number of HVG columns)
+// counter: one device word of scratch (zeroed here) for dynamic scheduling.
 int launch_project(const DevChunk &c, const int32_t *code, int64_t d, const DevScale &t, const double *V, int k,
-                   float *out, int by_span, cudaStream_t st);
+                   float *out, int by_span, unsigned int *counter, cudaStream_t st);
 // code[g] (g < c.n_gene_map): -1 dropped gene, sub_map[gene_map[g]] in [0, d)
 // for an HVG column, d for another kept gene.
 int launch_hvg_code(const DevChunk &c, const int32_t *sub_map, int64_t n_vars, int64_t d, int32_t *code,
                     cudaStream_t st);
+// Bytes of the code table of n_gene_map genes: int32 codes, then an int16
+// copy (16-byte aligned, zero-padded to a multiple of 8 entries).
+size_t hvg_code_bytes(int64_t n_gene_map);
+__host__ __device__ inline const int16_t *codes16(const int32_t *code, int64_t n_gene_map) {
+    return reinterpret_cast<const int16_t *>(code + round_up(n_gene_map, 4));
+}
+// Block-wide copy of the int16 codes into shared memory with 16-byte loads.
+__device__ inline void copy_codes16(const int32_t *code, int64_t n_gene_map, int16_t *dst) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(codes16(code, n_gene_map));
+    uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+    const int64_t n = round_up(n_gene_map, 8) / 8;
+    for (int64_t j = threadIdx.x; j < n; j += blockDim.x) d4[j] = __ldg(src + j);
+}
 // Largest dynamic shared memory a kernel here asks for (bytes).
-constexpr int kMaxSmem = 220 * 1024;
+constexpr int kMaxSmem = 227 * 1024;
 bool codes_in_smem(int64_t n_gene_map, int64_t d, size_t other_smem);
 int launch_scale_bias(const double *mean, const double *std, double mv, int64_t d, double *bias, cudaStream_t st);
 
@@ -49,6 +66,7 @@ struct GramWork {
     void *tile;             // FP64: double; FP32: float; BF16X3: hi then lo (bf16)
     double *colsum_chunk;   // [d] FP64 column sums of S for the current tile
     int64_t *n_kept;        // [1] kept cells in the current tile
+    unsigned int *counter;  // [1] next tile row to densify (dynamic scheduling)
     float *part32;          // [d_pad * d_pad] FP32 partial (FP32 / BF16X3)
     double *shift;          // [d_pad] tile value of a zero entry: bias rounded to the tile's
                             // precision, so the (repeated) zeros are stored exactly

@@ -1,8 +1,9 @@
 // Warp-per-cell building blocks shared by the streaming kernels.
 //
-// One warp owns one cell (one span of the chunk).  Its entries are read in
-// segments of 32 consecutive entries (lane j holds entry s + j), several
-// segments per iteration so each warp keeps more loads in flight.  All
+// One warp owns one cell (one span of the chunk).  Its entries are read
+// either in segments of 32 consecutive entries (lane j holds entry s + j;
+// for_entries) or in 128-entry blocks of four consecutive entries per lane
+// with 16-byte loads (for_entries_x4, the single-pass kernels).  All
 // per-cell f64 sums equal the reference's entry-order sums
 // (src/kernels.rs:69-76, 170-183).  When every value of the cell is an
 // integer below 2^24 (raw counts) all partial sums are exact, so per-lane
@@ -80,6 +81,108 @@ __device__ __forceinline__ void for_entries_by(const DevChunk &c, int64_t lo, in
             f(m, x[u]);
         }
     }
+}
+
+// Four entries per lane: lane l of a 128-entry block visits entries
+// b + 4l .. b + 4l + 3 with one 16-byte load of gene ids and one of values,
+// so a block is read in entry order lane by lane.  Entries before the first
+// 16-byte boundary form a head block of at most 3 (lanes 0-2, one entry
+// each); a partial last block is read entry by entry.  When genes and
+// values do not share their alignment every block is read entry by entry.
+// The next block's loads are issued before the current block is processed.
+// f(m[4], x[4]) is called by all 32 lanes once per block; m = -1 marks
+// dropped genes and empty slots.
+template <bool LAST, class L, class F>
+__device__ __forceinline__ void for_entries_x4(const DevChunk &c, int64_t lo, int64_t hi, L &&lookup, F &&f) {
+    const int lane = lane_id();
+    int32_t m[4];
+    float x[4];
+    const uintptr_t ga = reinterpret_cast<uintptr_t>(c.genes), va = reinterpret_cast<uintptr_t>(c.values);
+    const bool vec = ((ga ^ va) & 15) == 0;
+    int64_t b = lo;
+    if (vec && lo < hi) {
+        const int64_t head = (int64_t)((16 - ((ga + 4 * (uintptr_t)lo) & 15)) & 15) / 4;
+        if (head > 0) {
+            const int64_t hb = lo + head < hi ? lo + head : hi;
+            const int64_t e = lo + lane;
+            if (lane < 3 && e < hb) {
+                const uint32_t g = LAST ? __ldcs(c.genes + e) : __ldg(c.genes + e);
+                x[0] = LAST ? __ldcs(c.values + e) : __ldg(c.values + e);
+                m[0] = (int64_t)g < c.n_gene_map ? lookup(g) : -1;
+            } else {
+                x[0] = 0.0f;
+                m[0] = -1;
+            }
+            m[1] = m[2] = m[3] = -1;
+            x[1] = x[2] = x[3] = 0.0f;
+            f(m, x);
+            b = hb;
+        }
+    }
+    auto load = [&](int64_t bb, uint32_t (&g)[4], float (&v)[4]) {
+        const int64_t e = bb + 4 * lane;
+        if (vec && e + 3 < hi) {
+            const uint4 g4 = LAST ? __ldcs(reinterpret_cast<const uint4 *>(c.genes + e))
+                                  : __ldg(reinterpret_cast<const uint4 *>(c.genes + e));
+            const float4 x4 = LAST ? __ldcs(reinterpret_cast<const float4 *>(c.values + e))
+                                   : __ldg(reinterpret_cast<const float4 *>(c.values + e));
+            g[0] = g4.x;
+            g[1] = g4.y;
+            g[2] = g4.z;
+            g[3] = g4.w;
+            v[0] = x4.x;
+            v[1] = x4.y;
+            v[2] = x4.z;
+            v[3] = x4.w;
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const bool ok = e + u < hi;
+                g[u] = ok ? (LAST ? __ldcs(c.genes + e + u) : __ldg(c.genes + e + u)) : 0u;
+                v[u] = ok ? (LAST ? __ldcs(c.values + e + u) : __ldg(c.values + e + u)) : 0.0f;
+            }
+        }
+    };
+    if (b < hi) {
+        uint32_t ga_[4];
+        float xa_[4];
+        load(b, ga_, xa_);
+        for (; b < hi; b += 128) {
+            uint32_t gb_[4];
+            float xb_[4];
+            const bool more = b + 128 < hi;
+            if (more) load(b + 128, gb_, xb_);
+            const int64_t e = b + 4 * lane;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                x[u] = xa_[u];
+                m[u] = (e + u < hi && (int64_t)ga_[u] < c.n_gene_map) ? lookup(ga_[u]) : -1;
+            }
+            f(m, x);
+            if (more) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    ga_[u] = gb_[u];
+                    xa_[u] = xb_[u];
+                }
+            }
+        }
+    }
+}
+
+// Entry-order position of this lane's first selected entry within a block
+// visited by for_entries_x4, and the block's count of selected entries.
+__device__ __forceinline__ int block_rank4(const bool (&sel)[4], int &count) {
+    const unsigned lt = (1u << lane_id()) - 1u;
+    int before = 0;
+    count = 0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const unsigned bal = __ballot_sync(kFull, sel[u]);
+        before += __popc(bal & lt);
+        count += __popc(bal);
+    }
+    return before;
 }
 
 template <int U, bool LAST = true, class F>
