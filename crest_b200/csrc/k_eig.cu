@@ -49,12 +49,23 @@ __global__ void k_centre(const double *__restrict__ G, const double *__restrict_
     C[idx] = __ddiv_rn(__dsub_rn(G[a * d + b], __ddiv_rn(__dmul_rn(c[a], c[b]), n)), __dsub_rn(n, 1.0));
 }
 
-// total = sum_i cov[i][i] in index order (src/kernels.rs:323)
-__global__ void k_trace(const double *__restrict__ C, int64_t d, double *total) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// total = sum_i cov[i][i] in index order (src/kernels.rs:323): the diagonal
+// is gathered 1024 entries at a time into shared memory by the whole block,
+// then added up in order by one thread.
+__global__ void __launch_bounds__(1024) k_trace(const double *__restrict__ C, int64_t d, double *total) {
+    __shared__ double diag[1024];
     double s = 0.0;
-    for (int64_t i = 0; i < d; ++i) s = __dadd_rn(s, C[i * d + i]);
-    *total = s;
+    for (int64_t i0 = 0; i0 < d; i0 += 1024) {
+        const int64_t i = i0 + threadIdx.x;
+        if (i < d) diag[threadIdx.x] = C[i * d + i];
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int64_t n = d - i0 < 1024 ? d - i0 : 1024;
+            for (int64_t j = 0; j < n; ++j) s = __dadd_rn(s, diag[j]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = s;
 }
 
 // ------------------------------------------------------------------ GEMM
@@ -188,13 +199,14 @@ int gemm(const Gemm &g, GemmWs &w, cudaStream_t st) {
 // partition the indices, so A' = J^T A J splits into independent 2x2 blocks
 // (rows of pair i, columns of pair j): each thread updates whole blocks,
 // R_i^T M R_j, and one round costs two barriers.  A rotation is skipped when
-// |A_pq| <= eps sqrt(|A_pp A_qq|) (or below 1e-18 ||A||_F); the solver stops
+// |A_pq| <= n u sqrt(|A_pp A_qq|), u = 2^-52 (or below 1e-18 ||A||_F): below
+// that level a rotation only moves rounding noise around.  The solver stops
 // after a sweep without rotations.  The rotations accumulate in V (shared
 // memory when n <= 112, else the n x n global scratch Vwork).  The padding
 // row/column never couples, so the leading n_in x n_in block of V holds the
 // eigenvectors.  On exit: vals[i] = A_ii, Vout (n_in x n_in, col-major).
 template <bool V_SMEM>
-__global__ void __launch_bounds__(1024) k_jacobi(const double *__restrict__ Ain, int n_in, int n, double *Vwork,
+__global__ void __launch_bounds__(512) k_jacobi(const double *__restrict__ Ain, int n_in, int n, double *Vwork,
                                                  double *Vout, double *vals, int max_sweeps, int *sweeps_out) {
     extern __shared__ double S[];
     const int ld = n + 1;
@@ -227,7 +239,7 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double *__restrict__ Ain,
     }
     __syncthreads();
     const int half = n / 2;
-    const double eps = 0x1.0p-52;
+    const double eps = (double)n * 0x1.0p-52;
     int sweep = 0;
     for (; sweep < max_sweeps; ++sweep) {
         for (int r = 0; r < n - 1; ++r) {
@@ -251,39 +263,56 @@ __global__ void __launch_bounds__(1024) k_jacobi(const double *__restrict__ Ain,
                 qq_[i] = q;
             }
             __syncthreads();
-            // 2x2 blocks: rows of pair bi, columns of pair bj
-            for (int w = tid; w < half * half; w += nt) {
-                const int bi = w % half, bj = w / half;
-                const double si = sn_[bi], sj = sn_[bj];
-                if (si == 0.0 && sj == 0.0) continue;
-                const double ci = cs_[bi], cj = cs_[bj];
-                const int p = pp_[bi], q = qq_[bi], u = pp_[bj], v = qq_[bj];
-                const double m00 = S[p + u * ld], m01 = S[p + v * ld], m10 = S[q + u * ld], m11 = S[q + v * ld];
-                // rows: [c -s; s c] M
-                const double r00 = ci * m00 - si * m10, r01 = ci * m01 - si * m11;
-                const double r10 = si * m00 + ci * m10, r11 = si * m01 + ci * m11;
-                // columns: R [c s; -s c]
-                double n00 = cj * r00 - sj * r01, n01 = sj * r00 + cj * r01;
-                double n10 = cj * r10 - sj * r11, n11 = sj * r10 + cj * r11;
-                if (bi == bj) {  // the rotated pair itself: zero by construction
-                    n01 = 0.0;
-                    n10 = 0.0;
+            // Warp w owns the row pairs bi = w, w + nw, ...; lane l owns the
+            // column pairs bj = l, l + 32, ... and the rows j = l, l + 32, ...
+            // of V, so every rotation parameter is read once into registers.
+            {
+                const int lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+                double cj[3], sj[3];
+                int uj[3], vj[3];
+#pragma unroll
+                for (int t = 0; t < 3; ++t) {
+                    const int bj = lane + 32 * t;
+                    const bool in = bj < half;
+                    cj[t] = in ? cs_[bj] : 1.0;
+                    sj[t] = in ? sn_[bj] : 0.0;
+                    uj[t] = in ? pp_[bj] : 0;
+                    vj[t] = in ? qq_[bj] : 0;
                 }
-                S[p + u * ld] = n00;
-                S[p + v * ld] = n01;
-                S[q + u * ld] = n10;
-                S[q + v * ld] = n11;
-            }
-            // V <- V J (columns of each rotated pair)
-            for (int w = tid; w < half * n; w += nt) {
-                const int i = w / n, j = w % n;
-                const double s = sn_[i];
-                if (s == 0.0) continue;
-                const double c = cs_[i];
-                const int p = pp_[i], q = qq_[i];
-                const double vx = V[j + (int64_t)p * n], vy = V[j + (int64_t)q * n];
-                V[j + (int64_t)p * n] = c * vx - s * vy;
-                V[j + (int64_t)q * n] = s * vx + c * vy;
+                for (int bi = wid; bi < half; bi += nw) {
+                    const double ci = cs_[bi], si = sn_[bi];
+                    const int p = pp_[bi], q = qq_[bi];
+#pragma unroll
+                    for (int t = 0; t < 3; ++t) {
+                        const int bj = lane + 32 * t;
+                        if (bj >= half || (si == 0.0 && sj[t] == 0.0)) continue;
+                        const int u = uj[t], v = vj[t];
+                        const double m00 = S[p + u * ld], m01 = S[p + v * ld];
+                        const double m10 = S[q + u * ld], m11 = S[q + v * ld];
+                        // rows: [c -s; s c] M
+                        const double r00 = ci * m00 - si * m10, r01 = ci * m01 - si * m11;
+                        const double r10 = si * m00 + ci * m10, r11 = si * m01 + ci * m11;
+                        // columns: R [c s; -s c]
+                        double n00 = cj[t] * r00 - sj[t] * r01, n01 = sj[t] * r00 + cj[t] * r01;
+                        double n10 = cj[t] * r10 - sj[t] * r11, n11 = sj[t] * r10 + cj[t] * r11;
+                        if (bi == bj) {  // the rotated pair itself: zero by construction
+                            n01 = 0.0;
+                            n10 = 0.0;
+                        }
+                        S[p + u * ld] = n00;
+                        S[p + v * ld] = n01;
+                        S[q + u * ld] = n10;
+                        S[q + v * ld] = n11;
+                    }
+                    // V <- V J for the columns of pair bi
+                    if (si != 0.0) {
+                        for (int j = lane; j < n; j += 32) {
+                            const double vx = V[j + (int64_t)p * n], vy = V[j + (int64_t)q * n];
+                            V[j + (int64_t)p * n] = ci * vx - si * vy;
+                            V[j + (int64_t)q * n] = si * vx + ci * vy;
+                        }
+                    }
+                }
             }
             __syncthreads();
         }
@@ -308,11 +337,11 @@ int jacobi(const double *A, int n_in, double *Vwork, double *V, double *vals, in
     if (n <= kJacobiSmemV) {
         const size_t smem = sizeof(double) * ((size_t)n * (n + 1) + (size_t)n * n);
         CREST_TRY(ensure_smem_attr((const void *)k_jacobi<true>, (size_t)smem));
-        k_jacobi<true><<<1, 1024, smem, st>>>(A, n_in, n, nullptr, V, vals, 40, sweeps);
+        k_jacobi<true><<<1, 512, smem, st>>>(A, n_in, n, nullptr, V, vals, 40, sweeps);
     } else {
         const size_t smem = sizeof(double) * (size_t)n * (size_t)(n + 1);
         CREST_TRY(ensure_smem_attr((const void *)k_jacobi<false>, (size_t)smem));
-        k_jacobi<false><<<1, 1024, smem, st>>>(A, n_in, n, Vwork, V, vals, 40, sweeps);
+        k_jacobi<false><<<1, 512, smem, st>>>(A, n_in, n, Vwork, V, vals, 40, sweeps);
     }
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
@@ -462,16 +491,23 @@ __global__ void __launch_bounds__(1024) k_cgs2(double *Q, int64_t d, int j0, int
 // scaling leaves the span unchanged and removes the norm disparity a
 // Chebyshev filter creates), shifted by shift_coef * ||B'||_2 (bounded by
 // trace(B') = p), and factored B' = L L^T.  Rinv = D L^-T (upper triangular),
-// so Y Rinv has orthonormal columns.  One CTA, L and L^-1 in shared memory.
-// *fail = 1 when a column is zero or a pivot is not positive.
-__global__ void __launch_bounds__(1024) k_chol_inv(const double *__restrict__ B, int p, double shift_coef,
-                                                   double *__restrict__ Rinv, int *fail) {
+// so Y Rinv has orthonormal columns.  One CTA; L, L^-1 and a 16-row panel in
+// shared memory.  Both the factorisation and the inverse go by 16 x 16
+// blocks: the diagonal block by one warp, the panel and the trailing update
+// by the whole block, three barriers per block column.  *fail = 1 (and
+// Rinv = I, leaving Y unchanged) when a column is zero or a pivot is not
+// positive.
+constexpr int kCholNb = 16;
+
+__global__ void __launch_bounds__(512) k_chol_inv(const double *__restrict__ B, int p, double shift_coef,
+                                                  double *__restrict__ Rinv, int *fail) {
     extern __shared__ double sm[];
-    double *L = sm;                    // p x p, col-major
-    double *X = sm + (size_t)p * p;    // L^-1, col-major
+    double *L = sm;                     // p x p, col-major (lower triangle used)
+    double *X = sm + (size_t)p * p;     // L^-1, col-major
+    double *T = X + (size_t)p * p;      // kCholNb x p panel
     __shared__ double dsc[kJacobiMax];
     __shared__ int bad;
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5;
     if (tid == 0) bad = 0;
     __syncthreads();
     for (int i = tid; i < p; i += nt) {
@@ -487,36 +523,81 @@ __global__ void __launch_bounds__(1024) k_chol_inv(const double *__restrict__ B,
         X[w] = 0.0;
     }
     __syncthreads();
-    for (int k = 0; k < p; ++k) {
-        if (tid == 0) {
-            const double dk = L[k + k * p];
-            if (!(dk > 0.0)) bad = 1;
-            L[k + k * p] = dk > 0.0 ? sqrt(dk) : 1.0;
+    // ---- B' = L L^T, right-looking by block columns
+    for (int k0 = 0; k0 < p; k0 += kCholNb) {
+        const int kb = min(kCholNb, p - k0);
+        if (wid == 0) {  // diagonal block, unblocked, lane i owns row k0 + i
+            for (int j = 0; j < kb; ++j) {
+                const int jj = k0 + j;
+                double piv = L[jj + jj * p];
+                if (!(piv > 0.0)) {
+                    if (lane == 0) bad = 1;
+                    piv = 1.0;
+                }
+                const double r = sqrt(piv);
+                __syncwarp();
+                if (lane == j) L[jj + jj * p] = r;
+                if (lane > j && lane < kb) L[k0 + lane + jj * p] /= r;
+                __syncwarp();
+                if (lane > j && lane < kb) {
+                    const int i = k0 + lane;
+                    const double lij = L[i + jj * p];
+                    for (int c = j + 1; c <= lane; ++c) L[i + (k0 + c) * p] -= lij * L[k0 + c + jj * p];
+                }
+                __syncwarp();
+            }
         }
         __syncthreads();
-        const double lkk = L[k + k * p];
-        for (int i = k + 1 + tid; i < p; i += nt) L[i + k * p] /= lkk;
+        // panel below the diagonal block: L21 = A21 L11^-T, one row per thread
+        for (int i = k0 + kb + tid; i < p; i += nt) {
+            for (int j = 0; j < kb; ++j) {
+                double v = L[i + (k0 + j) * p];
+                for (int t = 0; t < j; ++t) v -= L[i + (k0 + t) * p] * L[k0 + j + (k0 + t) * p];
+                L[i + (k0 + j) * p] = v / L[k0 + j + (k0 + j) * p];
+            }
+        }
         __syncthreads();
-        const int m = p - k - 1;
-        for (int w = tid; w < m * m; w += nt) {
-            const int i = k + 1 + w % m, j = k + 1 + w / m;
-            if (i >= j) L[i + j * p] -= L[i + k * p] * L[j + k * p];
+        // trailing lower triangle: A22 -= L21 L21^T
+        const int r0 = k0 + kb, rem = p - r0;
+        for (int w = tid; w < rem * rem; w += nt) {
+            const int i = r0 + w % rem, j = r0 + w / rem;
+            if (i < j) continue;
+            double v = L[i + j * p];
+            for (int t = 0; t < kb; ++t) v -= L[i + (k0 + t) * p] * L[j + (k0 + t) * p];
+            L[i + j * p] = v;
         }
         __syncthreads();
     }
-    // X = L^-1 by forward substitution, one column per thread
-    for (int c = tid; c < p; c += nt) {
-        for (int i = c; i < p; ++i) {
-            double v = (i == c) ? 1.0 : 0.0;
-            for (int k = c; k < i; ++k) v -= L[i + k * p] * X[k + c * p];
-            X[i + c * p] = v / L[i + i * p];
+    // ---- X = L^-1 by block rows: X_II = L_II^-1, X_IC = -X_II sum_K L_IK X_KC
+    for (int i0 = 0; i0 < p; i0 += kCholNb) {
+        const int ib = min(kCholNb, p - i0);
+        if (wid == 0 && lane < ib) {  // diagonal block, lane c owns column i0 + c
+            const int c = lane;
+            for (int i = c; i < ib; ++i) {
+                double v = (i == c) ? 1.0 : 0.0;
+                for (int t = c; t < i; ++t) v -= L[i0 + i + (i0 + t) * p] * X[i0 + t + (i0 + c) * p];
+                X[i0 + i + (i0 + c) * p] = v / L[i0 + i + (i0 + i) * p];
+            }
         }
+        for (int w = tid; w < ib * i0; w += nt) {  // T[ii][c] = sum_{t=c}^{i0-1} L[i0+ii][t] X[t][c]
+            const int ii = w % ib, c = w / ib;
+            double v = 0.0;
+            for (int t = c; t < i0; ++t) v += L[i0 + ii + t * p] * X[t + c * p];
+            T[ii + c * kCholNb] = v;
+        }
+        __syncthreads();
+        for (int w = tid; w < ib * i0; w += nt) {
+            const int ii = w % ib, c = w / ib;
+            double v = 0.0;
+            for (int t = 0; t <= ii; ++t) v += X[i0 + ii + (i0 + t) * p] * T[t + c * kCholNb];
+            X[i0 + ii + c * p] = -v;
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    // Rinv = D (L^-1)^T
+    // Rinv = D (L^-1)^T, or the identity (Y left as it is) when the factor failed
     for (int w = tid; w < p * p; w += nt) {
         const int r = w % p, c = w / p;
-        Rinv[w] = dsc[r] * X[c + r * p];
+        Rinv[w] = bad ? (r == c ? 1.0 : 0.0) : dsc[r] * X[c + r * p];
     }
     if (tid == 0 && bad) *fail = 1;
 }
@@ -644,8 +725,11 @@ int orthonormalise(EigWork &w, double *Y, int64_t d, int j0, int q, bool shifted
     double *B = w.H.as<double>();
     double *Rinv = w.Q.as<double>();
     int *fail = w.fail.as<int>();
-    const size_t csmem = sizeof(double) * 2 * (size_t)q * q;
+    const size_t csmem = sizeof(double) * (2 * (size_t)q * q + (size_t)kCholNb * q);
     CREST_TRY(ensure_smem_attr((const void *)k_chol_inv, (size_t)csmem));
+    CREST_CUDA_TRY(cudaMemsetAsync(fail, 0, sizeof(int), st));
+    // all passes are queued without a host round trip: a failed factor leaves
+    // the block unchanged and raises the flag, checked once at the end
     const int passes = shifted ? 3 : 2;
     for (int pass = 0; pass < passes; ++pass) {
         if (j0 > 0) {  // remove the locked directions (twice for orthogonality)
@@ -657,23 +741,21 @@ int orthonormalise(EigWork &w, double *Y, int64_t d, int j0, int q, bool shifted
         CREST_TRY(gemm(Gemm{q, q, D, Ya, D, 1, Ya, D, B, q, 1.0, nullptr, 0.0, nullptr, 0.0}, w.g, st));
         // shift = 11 (d q + q (q + 1)) u ||B'||_2 on the first pass of the shifted form
         const double shift_coef = (shifted && pass == 0) ? 11.0 * ((double)d * q + (double)q * (q + 1)) * 0x1.0p-53 : 0.0;
-        CREST_CUDA_TRY(cudaMemsetAsync(fail, 0, sizeof(int), st));
         {
             prof::Scope ps("eig_cholqr", st);
-            k_chol_inv<<<1, 1024, csmem, st>>>(B, q, shift_coef, Rinv, fail);
+            k_chol_inv<<<1, 512, csmem, st>>>(B, q, shift_coef, Rinv, fail);
         }
         CREST_CUDA_TRY(cudaGetLastError());
-        int hf = 0;
-        CREST_CUDA_TRY(cudaMemcpyAsync(&hf, fail, sizeof(int), cudaMemcpyDeviceToHost, st));
-        CREST_CUDA_TRY(cudaStreamSynchronize(st));
-        if (hf) {
-            prof::Scope ps("eig_cgs2", st);
-            k_cgs2<<<1, 1024, sizeof(double) * (size_t)(j0 + q + 32), st>>>(Y, d, j0, j0 + q, seed + pass);
-            CREST_CUDA_TRY(cudaGetLastError());
-            return CREST_OK;
-        }
         CREST_TRY(gemm(Gemm{D, q, q, Ya, D, 0, Rinv, q, T, D, 1.0, nullptr, 0.0, nullptr, 0.0}, w.g, st));
         CREST_CUDA_TRY(cudaMemcpyAsync(Ya, T, sizeof(double) * (size_t)d * q, cudaMemcpyDeviceToDevice, st));
+    }
+    int hf = 0;
+    CREST_CUDA_TRY(cudaMemcpyAsync(&hf, fail, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CREST_CUDA_TRY(cudaStreamSynchronize(st));
+    if (hf) {  // rank-deficient block: Gram-Schmidt with random replacements
+        prof::Scope ps("eig_cgs2", st);
+        k_cgs2<<<1, 1024, sizeof(double) * (size_t)(j0 + q + 32), st>>>(Y, d, j0, j0 + q, seed);
+        CREST_CUDA_TRY(cudaGetLastError());
     }
     return CREST_OK;
 }
@@ -697,7 +779,7 @@ int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_
         k_centre<<<(unsigned)ceil_div(d * d, 256), 256, 0, st>>>(G, colsum, d, nf, C);
     }
     CREST_CUDA_TRY(cudaGetLastError());
-    k_trace<<<1, 32, 0, st>>>(C, d, out_total);
+    k_trace<<<1, 1024, 0, st>>>(C, d, out_total);
     CREST_CUDA_TRY(cudaGetLastError());
     if (stats) *stats = EigStats{0, 1, 0.0};
     if (k == 0) return CREST_OK;
