@@ -9,7 +9,7 @@
 // memory, round-robin parallel ordering).
 //
 // d > 160: Chebyshev-filtered subspace iteration (Zhou & Saad 2007) with
-// locking, on a block of p = k + 32 (rounded to 16) vectors:
+// locking, on a block of p = k + 14 (rounded up to 16) vectors:
 //  * a short Lanczos run (full re-orthogonalisation) brackets the spectrum;
 //    the filter damps [lambda_min, a] with a = the smallest active Ritz
 //    value, so eigenvalues far from zero (scaled single-cell data: a dense
@@ -812,7 +812,7 @@ int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_
         return CREST_OK;
     }
 
-    int p = (int)round_up(k + 32, 16);
+    int p = (int)round_up(k + 14, 16);
     if (p > kJacobiSmemV) p = kJacobiSmemV;
     if (p > d) p = (int)d;
     CREST_REQUIRE(k <= p - 8, CREST_EINVAL, "n_comps=%lld too large for the block eigensolver (max %d)",
