@@ -204,6 +204,29 @@ int crest_pca_project(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
                       int64_t n_rows, float *out, int32_t out_mem);
 int crest_pca_stats_get(const crest_pca *p, crest_pca_stats *stats);
 
+/* ------------------------------------------------------- differentiation
+ * The normalise -> log1p -> scale -> project map of a CSR matrix over d
+ * genes (HVG columns already selected) and its gradient, for the autograd
+ * hook of the Python package.  No counterpart in the reference; the forward
+ * arithmetic is its transform (src/kernels.rs:79-82, 209-219, 352-371) with
+ * the normalisation written as a per-cell size factor that DIVIDES:
+ *   y = x / sf[c] (f32), l = log1pf(y), s = clip((l - mean)/std) - clip(-mean/std),
+ *   scores[c, :] = sum over the cell's entries of s W[g, :]  (f64 sums, f32 out).
+ * All pointers are DEVICE memory of the current device: indptr i64[n+1]
+ * (indptr[0] = 0), indices i32[nnz] in [0, d), values f32[nnz], size_factors
+ * f32[n], W f32[d, k] row-major (1 <= k <= 128), mean/std f64[d],
+ * scores f32[n, k].  A gene id outside [0, d) returns CREST_EINVAL. */
+int crest_fused_forward(const int64_t *indptr, const int32_t *indices, const float *values, int64_t n,
+                        int64_t d, const float *size_factors, const float *W, int64_t k,
+                        const double *mean, const double *std, double max_value, float *scores);
+/* Gradients of L given grad_scores = dL/dscores (f32[n, k]): grad_values
+ * f32[nnz], grad_sf f32[n], grad_W f32[d, k] (all overwritten).  log1p and
+ * the scaled values are recomputed, not stored by the forward. */
+int crest_fused_backward(const int64_t *indptr, const int32_t *indices, const float *values, int64_t n,
+                         int64_t d, const float *size_factors, const float *W, int64_t k,
+                         const double *mean, const double *std, double max_value,
+                         const float *grad_scores, float *grad_values, float *grad_sf, float *grad_W);
+
 /* ---------------------------------------------------------------- timing
  * Optional per-kernel device timing with CUDA events around each launch on
  * its stream (no counterpart in the reference, which has no GPU code).

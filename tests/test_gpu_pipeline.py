@@ -119,7 +119,12 @@ def test_chunking_store_and_residency_invariance():
     c, inp, g = load_case("small")
     a = pipeline(frame(inp), c, "fp64")
     b = pipeline(frame(inp, residency="host"), c, "fp64")
-    assert np.array_equal(a.obsm["X_pca"], b.obsm["X_pca"])
+    # per-gene f64 statistics are summed with atomics (their order, like the
+    # reference's per-thread parts, is not fixed), so the scale parameters may
+    # differ in the last bits between runs: equal up to that
+    assert np.array_equal(a.var["highly_variable"].to_numpy(), b.var["highly_variable"].to_numpy())
+    assert max_angle(a.obsm["X_pca"], b.obsm["X_pca"]) <= 1e-4
+    assert aligned_rel_err(a.obsm["X_pca"], b.obsm["X_pca"]) <= 1e-6
     indptr, indices, data, n_genes, names = inp
     cells = np.repeat(np.arange(len(indptr) - 1), np.diff(indptr)).astype(np.uint32)
     t = cb.BioFrame.from_triplets(cells, indices, data, len(indptr) - 1, n_genes,
