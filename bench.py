@@ -239,13 +239,6 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ GPU arm
-class DevArray:
-    """__cuda_array_interface__ view of a device pointer (for torch.distributed)."""
-
-    def __init__(self, ptr, n):
-        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 3}
-
-
 def main_gpu(args):
     import torch
     import crest_b200 as cb
@@ -259,7 +252,9 @@ def main_gpu(args):
     if ws > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        from crest_b200 import dist as cdist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        cdist.enable()  # per-gene sums and the Gram are summed over ranks
 
     wl, (indptr, indices, data), gen_s = build_inputs(args, rank, "gpu")
     from crest_b200 import synth
@@ -277,16 +272,11 @@ def main_gpu(args):
     def step(plan):
         plan.accumulate(dm, P["cmap"], P["gmap"], P["target"], P["log"], P["sub"], P["n_vars"], P["scale"])
         n_tot = n_rows
-        if dist is not None:
+        if dist is not None:  # one NCCL sum of the FP64 accumulators and the cell count
             gp, cp = plan.accumulators()
-            g = torch.as_tensor(DevArray(gp, P["d"] * P["d"]), device="cuda")
-            c = torch.as_tensor(DevArray(cp, P["d"]), device="cuda")
-            dist.all_reduce(g)
-            dist.all_reduce(c)
-            nt = torch.tensor([n_rows], dtype=torch.float64, device="cuda")
-            dist.all_reduce(nt)
-            torch.cuda.synchronize()
-            n_tot = int(nt.item())
+            cdist.sum_device(gp, P["d"] * P["d"])
+            cdist.sum_device(cp, P["d"])
+            n_tot = cdist.sum_count(n_rows)
         plan.solve(n_tot, k)
         plan.project(dm, P["cmap"], P["gmap"], P["target"], P["log"], P["sub"], P["n_vars"], P["scale"], n_rows,
                      device_ptr=X.data_ptr())

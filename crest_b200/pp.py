@@ -17,11 +17,11 @@ from typing import Optional
 import numpy as np
 import pandas as pd
 
-from . import _lib, _native
+from . import _lib, _native, dist
 from .core import BioFrame
 
 __all__ = ["calculate_qc_metrics", "filter_cells", "filter_genes", "normalize_total", "log1p", "scale",
-           "gene_stats", "highly_variable_genes"]
+           "gene_stats", "highly_variable_genes", "hvg_from_stats"]
 
 
 # --------------------------------------------------------------------------- QC
@@ -45,7 +45,8 @@ def _qc_sums(bf: BioFrame, flag: np.ndarray):
     else:
         for ctx in bf.iter_ctx(transform=False):
             _native.qc(*ctx, flag, ct, cn, cf, gn, gt)
-    return ct, cn, cf, gn, gt
+    # per-gene sums cover the cells of every rank (identity in one process)
+    return ct, cn, cf, dist.sum_host(gn), dist.sum_host(gt)
 
 
 def calculate_qc_metrics(bf: BioFrame, mito_prefix: Optional[str] = "MT-", inplace: bool = True):
@@ -141,7 +142,7 @@ def gene_stats(bf: BioFrame) -> np.ndarray:
     else:
         for ctx in bf.iter_ctx():
             _native.gene_stats(*ctx, out)
-    return out
+    return dist.sum_host(out)
 
 
 def _mean_var(s1: np.ndarray, s2: np.ndarray, n: int):
@@ -174,15 +175,28 @@ def highly_variable_genes(bf: BioFrame, n_top_genes: Optional[int] = None, flavo
         raise NotImplementedError("flavor='seurat_v3' is outside this package's hot path")
     if batch_key is not None:
         raise NotImplementedError("batch_key is supported for flavor='seurat_v3' only")
-    n = bf.n_obs
-    st = gene_stats(bf)
+    cols = hvg_from_stats(gene_stats(bf), dist.sum_count(bf.n_obs), n_top_genes, flavor, n_bins, min_mean,
+                          max_mean, min_disp, max_disp)
+    for name, v in cols.items():
+        bf.var[name] = v
+    bf.uns["hvg"] = {"flavor": flavor, "ops": list(bf.ops)}
+    if subset:
+        return bf._subset(var_mask=cols["highly_variable"])
+    return bf
+
+
+def hvg_from_stats(st: np.ndarray, n: int, n_top_genes: Optional[int] = None, flavor: str = "seurat",
+                   n_bins: int = 20, min_mean: float = 0.0125, max_mean: float = 3.0, min_disp: float = 0.5,
+                   max_disp: float = np.inf) -> dict:
+    """The host-side HVG math of crest/pp.py:201-292 from per-gene statistics
+    ``st`` (n_vars x 5, :func:`gene_stats`) over ``n`` cells: the var columns."""
+    if flavor not in ("seurat", "cell_ranger"):
+        raise ValueError('flavor must be "seurat" or "cell_ranger"')
     mean_log, var_log = _mean_var(st[:, 0], st[:, 1], n)
     if flavor == "seurat":
         mean, var = _mean_var(st[:, 2], st[:, 3], n)
-    elif flavor == "cell_ranger":
-        mean, var = mean_log.copy(), var_log.copy()
     else:
-        raise ValueError('flavor must be "seurat" or "cell_ranger"')
+        mean, var = mean_log.copy(), var_log.copy()
     mean = mean.copy()
     mean[mean == 0] = 1e-12
     with np.errstate(divide="ignore", invalid="ignore"):
@@ -221,7 +235,7 @@ def highly_variable_genes(bf: BioFrame, n_top_genes: Optional[int] = None, flavo
 
     if n_top_genes is not None:
         ok = disp_norm[~np.isnan(disp_norm)]
-        k = min(n_top_genes, ok.size, bf.n_vars)
+        k = min(n_top_genes, ok.size, st.shape[0])
         cutoff = np.sort(ok)[::-1][k - 1]
         hv = np.nan_to_num(disp_norm, nan=-np.inf) >= cutoff
     else:
@@ -230,11 +244,5 @@ def highly_variable_genes(bf: BioFrame, n_top_genes: Optional[int] = None, flavo
 
     std_log = np.sqrt(var_log)
     std_log[std_log == 0] = 1.0
-    cols = {"means": mean, "dispersions": disp, "dispersions_norm": disp_norm, "highly_variable": hv,
+    return {"means": mean, "dispersions": disp, "dispersions_norm": disp_norm, "highly_variable": hv,
             "mean_log": mean_log, "std_log": std_log, "n_cells_expr": st[:, 4].astype(np.int64)}
-    for name, v in cols.items():
-        bf.var[name] = v
-    bf.uns["hvg"] = {"flavor": flavor, "ops": list(bf.ops)}
-    if subset:
-        return bf._subset(var_mask=hv)
-    return bf

@@ -9,7 +9,7 @@ from typing import Optional
 
 import numpy as np
 
-from . import _lib, _native
+from . import _lib, _native, dist
 from .core import BioFrame
 from .pp import _mean_var, gene_stats
 
@@ -23,7 +23,7 @@ def _scale_params(bf: BioFrame, mask: np.ndarray):
         mean, std = bf.var["mean_log"].to_numpy(), bf.var["std_log"].to_numpy()
     else:
         st = gene_stats(bf)
-        mean, var = _mean_var(st[:, 0], st[:, 1], bf.n_obs)
+        mean, var = _mean_var(st[:, 0], st[:, 1], dist.sum_count(bf.n_obs))
         std = np.sqrt(var)
         std[std == 0] = 1.0
     return np.ascontiguousarray(mean[mask], np.float64), np.ascontiguousarray(std[mask], np.float64)
@@ -126,7 +126,8 @@ def pca(bf: BioFrame, n_comps: int = 50, use_highly_variable: Optional[bool] = N
     if scale:
         mean, std = _scale_params(bf, mask)
     mv = float(max_value or 0.0)
-    n = bf.n_obs
+    n_local = bf.n_obs
+    n = dist.sum_count(n_local)  # cells over all ranks (the covariance's n)
     k = min(n_comps, d, n - 1)
 
     dm = bf.device_matrix()
@@ -138,9 +139,13 @@ def pca(bf: BioFrame, n_comps: int = 50, use_highly_variable: Optional[bool] = N
         plan = PcaPlan(d, gram_precision)
         try:
             plan.accumulate(dm, cmap, gmap, target, log, sub, bf.n_vars, t)
+            if dist.active():  # one sum of the FP64 accumulators before the replicated solve
+                g_dev, c_dev = plan.accumulators()
+                dist.sum_device(g_dev, d * d)
+                dist.sum_device(c_dev, d)
             plan.solve(n, k)
             variance, loadings, total, colsum = plan.results()
-            X = plan.project(dm, cmap, gmap, target, log, sub, bf.n_vars, t, n)
+            X = plan.project(dm, cmap, gmap, target, log, sub, bf.n_vars, t, n_local)
             stats = plan.stats()
         finally:
             plan.close()
@@ -150,10 +155,11 @@ def pca(bf: BioFrame, n_comps: int = 50, use_highly_variable: Optional[bool] = N
         colsum = np.zeros(d, np.float64)
         for ctx in bf.iter_ctx():
             _native.gram_accumulate(*ctx, sub, gram, colsum, scale, mean, std, mv, precision=gram_precision)
+        gram, colsum = dist.sum_host(gram), dist.sum_host(colsum)
         variance, loadings, total = _native.pca_from_gram(gram, colsum, n, k)
         del gram
         shift = (colsum / n) @ loadings
-        X = np.empty((n, k), np.float32)
+        X = np.empty((n_local, k), np.float32)
         X[:] = -shift.astype(np.float32)
         for ctx in bf.iter_ctx():
             _native.project(*ctx, sub, loadings, X, scale, mean, std, mv)
