@@ -26,7 +26,10 @@
 // Stops when every wanted residual ||C v - theta v|| <= tol * theta_1.
 #include <math.h>
 
+#include <cublas_v2.h>
+
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "kernels.cuh"
@@ -167,8 +170,58 @@ struct GemmWs {
     DevBuf ws;
 };
 
+// O = beta X + gamma Y (either may be NULL), element-wise over M x N.
+__global__ void k_axpby(Gemm g) {
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)g.M * g.N) return;
+    const int m = (int)(idx % g.M), n = (int)(idx / g.M);
+    const int64_t o = m + (int64_t)n * g.ldo;
+    double v = 0.0;
+    if (g.X) v += g.beta * g.X[o];
+    if (g.Y) v += g.gamma * g.Y[o];
+    g.O[o] = v;
+}
+
+// cuBLAS handle of the current device (created on first use).
+int blas_handle(cublasHandle_t *out) {
+    static std::mutex mu;
+    static cublasHandle_t h[64] = {};
+    int dev = 0;
+    CREST_CUDA_TRY(cudaGetDevice(&dev));
+    CREST_REQUIRE(dev >= 0 && dev < 64, CREST_ERUNTIME, "device index %d out of range", dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!h[dev]) {
+        const cublasStatus_t r = cublasCreate(&h[dev]);
+        CREST_REQUIRE(r == CUBLAS_STATUS_SUCCESS, CREST_ECUDA, "cublasCreate failed (%d)", (int)r);
+    }
+    *out = h[dev];
+    return CREST_OK;
+}
+
+// The filter's large products (C times a d x q block, d and K >= 512) go to
+// cuBLAS DGEMM; the epilogue's extra terms are formed first in O.
+int gemm_blas(const Gemm &g, cudaStream_t st) {
+    cublasHandle_t h;
+    CREST_TRY(blas_handle(&h));
+    CREST_REQUIRE(cublasSetStream(h, st) == CUBLAS_STATUS_SUCCESS, CREST_ECUDA, "cublasSetStream failed");
+    double beta = 0.0;
+    if (g.Y || (g.X && g.X != g.O)) {
+        k_axpby<<<(unsigned)ceil_div((int64_t)g.M * g.N, 256), 256, 0, st>>>(g);
+        CREST_CUDA_TRY(cudaGetLastError());
+        beta = 1.0;
+    } else if (g.X == g.O && g.X) {
+        beta = g.beta;
+    }
+    const cublasStatus_t r =
+        cublasDgemm(h, g.tA ? CUBLAS_OP_T : CUBLAS_OP_N, g.tB ? CUBLAS_OP_T : CUBLAS_OP_N, g.M, g.N, g.K, &g.alpha,
+                    g.A, g.lda, g.B, g.ldb, &beta, g.O, g.ldo);
+    CREST_REQUIRE(r == CUBLAS_STATUS_SUCCESS, CREST_ECUDA, "cublasDgemm failed (%d)", (int)r);
+    return CREST_OK;
+}
+
 int gemm(const Gemm &g, GemmWs &w, cudaStream_t st) {
     prof::Scope ps("eig_gemm_fp64", st);
+    if (g.M >= 512 && g.K >= 512) return gemm_blas(g, st);
     const int mt = (int)ceil_div(g.M, 64), nt = (int)ceil_div(g.N, 64);
     int ksplit = 1;
     if (g.K > 0) {
