@@ -29,6 +29,17 @@ struct crest_matrix {
     // per-pass staging
     crest::DevBuf cell_map, gene_map, flag, sub_map, code, counter, mean, std_, bias;
     crest::DevBuf out[5];
+    // gene-range index of a device-resident matrix (built on first use):
+    // range_state 0 = not built, 1 = rows sorted (index valid), -1 = unsorted
+    int range_state = 0;
+    int range_log2_s = 12, n_ranges = 0;
+    crest::DevBuf range_off, status;
+    int qc_integral = 1;  // cleared once the QC sweep meets a non-integral value
+    // per-cell kept-gene totals of a device-resident matrix for the gene_map
+    // they were formed with
+    crest::DevBuf totals;
+    std::vector<int32_t> totals_key;
+    bool totals_valid = false;
 };
 
 struct crest_pca {
@@ -157,6 +168,56 @@ int for_each_piece(crest_matrix *m, const DevChunk &proto, int64_t max_cells, F 
     return CREST_OK;
 }
 
+// The gene-range index of a device-resident matrix, built on first use;
+// false when the matrix is streamed or has a row that is not sorted.
+int range_index(crest_matrix *m, RangeIndex &ix, bool &ok) {
+    ok = false;
+    if (m->residency != CREST_MEM_DEVICE || m->n_cells == 0 || m->n_genes == 0) return CREST_OK;
+    if (m->range_state == 0) {
+        const int R = (int)std::max<int64_t>(2, ceil_div(m->n_genes, (int64_t)1 << m->range_log2_s));
+        CREST_TRY(m->range_off.ensure((size_t)m->n_cells * (R - 1) * sizeof(int32_t)));
+        CREST_TRY(m->status.ensure(sizeof(int)));
+        CREST_CUDA_TRY(cudaMemsetAsync(m->status.ptr, 0, sizeof(int), m->compute));
+        CREST_TRY(launch_range_index(m->d_indptr.as<int64_t>(), m->d_indices.as<uint32_t>(), m->n_cells,
+                                     m->range_log2_s, R, m->range_off.as<int32_t>(), m->status.as<int>(),
+                                     m->compute));
+        int unsorted = 0;
+        CREST_CUDA_TRY(cudaMemcpyAsync(&unsorted, m->status.ptr, sizeof(int), cudaMemcpyDeviceToHost, m->compute));
+        CREST_CUDA_TRY(cudaStreamSynchronize(m->compute));
+        m->n_ranges = R;
+        m->range_state = unsorted ? -1 : 1;
+        if (unsorted) m->range_off.release();
+    }
+    if (m->range_state != 1) return CREST_OK;
+    ix.log2_s = m->range_log2_s;
+    ix.n_ranges = m->n_ranges;
+    ix.off = m->range_off.as<int32_t>();
+    ok = true;
+    return CREST_OK;
+}
+
+// Per-cell kept-gene totals of a device-resident matrix for the staged
+// gene_map (cached until the map changes).
+int cell_totals(crest_matrix *m, const int32_t *gene_map, const DevChunk &proto, const double **out) {
+    const bool same = m->totals_valid && m->totals_key.size() == (size_t)m->n_genes &&
+                      std::equal(m->totals_key.begin(), m->totals_key.end(), gene_map);
+    if (!same) {
+        m->totals_valid = false;
+        CREST_TRY(m->totals.ensure(sizeof(double) * std::max<int64_t>(m->n_cells, 1)));
+        DevChunk c = proto;
+        c.genes = m->d_indices.as<uint32_t>();
+        c.values = m->d_data.as<float>();
+        c.first_cell = 0;
+        c.base = 0;
+        c.n_spans = m->n_cells;
+        CREST_TRY(launch_cell_totals(c, m->totals.as<double>(), m->compute));
+        m->totals_key.assign(gene_map, gene_map + m->n_genes);
+        m->totals_valid = true;
+    }
+    *out = m->totals.as<double>();
+    return CREST_OK;
+}
+
 __global__ void k_init_scores(const double *__restrict__ colsum, const double *__restrict__ V, int64_t d, int64_t k,
                               double n, double *__restrict__ shift) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -257,7 +318,9 @@ int crest_matrix_free(crest_matrix *m) {
         if (m->ev_ready[i]) cudaEventDestroy(m->ev_ready[i]);
         if (m->ev_free[i]) cudaEventDestroy(m->ev_free[i]);
     }
-    for (auto *b : {&m->cell_map, &m->gene_map, &m->flag, &m->sub_map, &m->mean, &m->std_, &m->bias}) b->release();
+    for (auto *b : {&m->cell_map, &m->gene_map, &m->flag, &m->sub_map, &m->mean, &m->std_, &m->bias, &m->range_off,
+                    &m->status, &m->totals})
+        b->release();
     for (auto &b : m->out) b.release();
     if (m->compute) cudaStreamDestroy(m->compute);
     if (m->copy) cudaStreamDestroy(m->copy);
@@ -288,9 +351,36 @@ int crest_matrix_qc(crest_matrix *m, const int64_t *cell_map, const int32_t *gen
     CREST_TRY(zeros<double>(m->out[4], n_vars, st));
     RowOut ro{m->out[0].as<double>(), m->out[1].as<uint32_t>(), m->out[2].as<double>()};
     const DevChunk proto = base_chunk(m, 0.0, 0);
-    CREST_TRY(for_each_piece(m, proto, m->n_cells, [&](const DevChunk &c) {
-        return launch_qc(c, m->flag.as<uint8_t>(), m->out[3].as<uint32_t>(), m->out[4].as<double>(), nullptr, &ro, st);
-    }));
+    RangeIndex ix;
+    bool swept = false;
+    CREST_TRY(range_index(m, ix, swept));
+    swept = swept && m->qc_integral;
+    if (swept) {  // gene-range sweep over the whole resident matrix
+        DevChunk c = proto;
+        c.genes = m->d_indices.as<uint32_t>();
+        c.values = m->d_data.as<float>();
+        c.n_spans = m->n_cells;
+        CREST_CUDA_TRY(cudaMemsetAsync(m->status.ptr, 0, sizeof(int), st));
+        CREST_TRY(launch_qc_sweep(c, ix, m->flag.as<uint8_t>(), m->out[3].as<uint32_t>(), m->out[4].as<double>(),
+                                  ro, m->status.as<int>(), st));
+        int status = 0;
+        CREST_CUDA_TRY(cudaMemcpyAsync(&status, m->status.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CREST_CUDA_TRY(cudaStreamSynchronize(st));
+        if (status) {  // a non-integral value: redo in entry order
+            m->qc_integral = 0;
+            swept = false;
+            CREST_TRY(zeros<double>(m->out[0], n_rows, st));
+            CREST_TRY(zeros<uint32_t>(m->out[1], n_rows, st));
+            CREST_TRY(zeros<double>(m->out[2], n_rows, st));
+            CREST_TRY(zeros<uint32_t>(m->out[3], n_vars, st));
+            CREST_TRY(zeros<double>(m->out[4], n_vars, st));
+        }
+    }
+    if (!swept)
+        CREST_TRY(for_each_piece(m, proto, m->n_cells, [&](const DevChunk &c) {
+            return launch_qc(c, m->flag.as<uint8_t>(), m->out[3].as<uint32_t>(), m->out[4].as<double>(), nullptr, &ro,
+                             st);
+        }));
     if (n_rows) {
         CREST_CUDA_TRY(cudaMemcpyAsync(cell_total, m->out[0].ptr, 8 * n_rows, cudaMemcpyDeviceToHost, st));
         CREST_CUDA_TRY(cudaMemcpyAsync(cell_ngenes, m->out[1].ptr, 4 * n_rows, cudaMemcpyDeviceToHost, st));
@@ -312,8 +402,21 @@ int crest_matrix_gene_stats(crest_matrix *m, const int64_t *cell_map, const int3
     cudaStream_t st = m->compute;
     CREST_TRY(zeros<double>(m->out[0], n_vars * 5, st));
     const DevChunk proto = base_chunk(m, target_sum, log1p);
-    CREST_TRY(for_each_piece(m, proto, m->n_cells,
-                             [&](const DevChunk &c) { return launch_gene_stats(c, m->out[0].as<double>(), st); }));
+    RangeIndex ix;
+    bool swept = false;
+    CREST_TRY(range_index(m, ix, swept));
+    if (swept) {  // gene-range sweep over the whole resident matrix
+        const double *total = nullptr;
+        if (target_sum > 0.0) CREST_TRY(cell_totals(m, gene_map, proto, &total));
+        DevChunk c = proto;
+        c.genes = m->d_indices.as<uint32_t>();
+        c.values = m->d_data.as<float>();
+        c.n_spans = m->n_cells;
+        CREST_TRY(launch_gene_stats_sweep(c, ix, total, m->out[0].as<double>(), st));
+    } else {
+        CREST_TRY(for_each_piece(m, proto, m->n_cells,
+                                 [&](const DevChunk &c) { return launch_gene_stats(c, m->out[0].as<double>(), st); }));
+    }
     if (n_vars) CREST_CUDA_TRY(cudaMemcpyAsync(out, m->out[0].ptr, 40 * n_vars, cudaMemcpyDeviceToHost, st));
     CREST_CUDA_TRY(cudaStreamSynchronize(st));
     return CREST_OK;

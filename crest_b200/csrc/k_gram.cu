@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(kDensifyWarps * 32, 1) k_densify(DevChunk c, c
         bool ok = true, ovf = false;
         int nq = 0;
         if (kept) {
-            for_entries_x4<true>(c, lo, hi, lookup, [&](const int32_t (&m)[4], const float (&x)[4]) {
+            for_entries_x4<true, kDensifyDepth>(c, lo, hi, lookup, [&](const int32_t (&m)[4], const float (&x)[4]) {
                 bool hv[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {

@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(kProjWarps * 32, 1) k_project(DevChunk c, cons
         double tsum = 0.0;
         bool ok = true, ovf = false;
         int nq = 0;
-        for_entries_x4<true>(c, lo, hi, lookup, [&](const int32_t (&m)[4], const float (&x)[4]) {
+        for_entries_x4<true, kProjDepth>(c, lo, hi, lookup, [&](const int32_t (&m)[4], const float (&x)[4]) {
             bool hv[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {

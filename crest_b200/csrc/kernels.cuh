@@ -25,6 +25,29 @@ struct RowOut {  // per-row QC results added at the cell's row (matrix API)
 int launch_qc(const DevChunk &c, const uint8_t *flag, uint32_t *gene_ncells, double *gene_total,
               const SpanOut *span, const RowOut *row, cudaStream_t st);
 int launch_gene_stats(const DevChunk &c, double *out, cudaStream_t st);
+// Gene-range index of a device-resident CSR matrix with rows sorted by gene
+// id: off[cell * (n_ranges - 1) + b - 1] = first entry of the row (relative
+// to its start) with gene >= b << log2_s, b = 1 .. n_ranges - 1.
+struct RangeIndex {
+    int log2_s;
+    int n_ranges;
+    const int32_t *off;
+};
+constexpr int kSweepThreads = 768;
+// Builds the index; sets *unsorted to 1 if some row is not sorted.
+int launch_range_index(const int64_t *indptr, const uint32_t *genes, int64_t n_cells, int log2_s, int n_ranges,
+                       int32_t *off, int *unsorted, cudaStream_t st);
+// Per-gene QC sums and per-row (t, n, f) of a piece whose spans are matrix
+// cells first_cell + i.  Integral values only: bit 1 of *status is set
+// otherwise and the results must be discarded.
+int launch_qc_sweep(const DevChunk &c, const RangeIndex &ix, const uint8_t *flag, uint32_t *gene_ncells,
+                    double *gene_total, const RowOut &row, int *status, cudaStream_t st);
+// gene_stats of a piece given its per-span kept-gene totals.
+int launch_gene_stats_sweep(const DevChunk &c, const RangeIndex &ix, const double *total, double *out,
+                            cudaStream_t st);
+// total[i] = sum of the kept-gene values of span i (normalisation total).
+int launch_cell_totals(const DevChunk &c, double *total, cudaStream_t st);
+
 // out row index: the cell's row, or the span index when by_span != 0
 // code: per-gene HVG codes from launch_hvg_code (d = number of HVG columns)
 // counter: one device word of scratch (zeroed here) for dynamic scheduling.
@@ -49,6 +72,10 @@ __device__ inline void copy_codes16(const int32_t *code, int64_t n_gene_map, int
 }
 // Largest dynamic shared memory a kernel here asks for (bytes).
 constexpr int kMaxSmem = 227 * 1024;
+// Blocks of 128 entries whose loads are in flight while one is processed
+// (for_entries_x4) in the densify and projection passes.
+constexpr int kDensifyDepth = 1;
+constexpr int kProjDepth = 1;
 bool codes_in_smem(int64_t n_gene_map, int64_t d, size_t other_smem);
 int launch_scale_bias(const double *mean, const double *std, double mv, int64_t d, double *bias, cudaStream_t st);
 

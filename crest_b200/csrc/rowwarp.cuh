@@ -89,10 +89,11 @@ __device__ __forceinline__ void for_entries_by(const DevChunk &c, int64_t lo, in
 // 16-byte boundary form a head block of at most 3 (lanes 0-2, one entry
 // each); a partial last block is read entry by entry.  When genes and
 // values do not share their alignment every block is read entry by entry.
-// The next block's loads are issued before the current block is processed.
+// The loads of the next D blocks are in flight while a block is processed
+// (D + 1 register buffers, indexed statically).
 // f(m[4], x[4]) is called by all 32 lanes once per block; m = -1 marks
 // dropped genes and empty slots.
-template <bool LAST, class L, class F>
+template <bool LAST, int D = 1, class L, class F>
 __device__ __forceinline__ void for_entries_x4(const DevChunk &c, int64_t lo, int64_t hi, L &&lookup, F &&f) {
     const int lane = lane_id();
     int32_t m[4];
@@ -143,29 +144,25 @@ __device__ __forceinline__ void for_entries_x4(const DevChunk &c, int64_t lo, in
             }
         }
     };
-    if (b < hi) {
-        uint32_t ga_[4];
-        float xa_[4];
-        load(b, ga_, xa_);
-        for (; b < hi; b += 128) {
-            uint32_t gb_[4];
-            float xb_[4];
-            const bool more = b + 128 < hi;
-            if (more) load(b + 128, gb_, xb_);
-            const int64_t e = b + 4 * lane;
+    constexpr int NB = D + 1;
+    uint32_t gq[NB][4];
+    float xq[NB][4];
+#pragma unroll
+    for (int k = 0; k < NB; ++k)
+        if (b + 128 * k < hi) load(b + 128 * k, gq[k], xq[k]);
+    for (; b < hi; b += 128 * NB) {
+#pragma unroll
+        for (int k = 0; k < NB; ++k) {
+            const int64_t bb = b + 128 * k;
+            if (bb >= hi) break;  // warp-uniform
+            const int64_t e = bb + 4 * lane;
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                x[u] = xa_[u];
-                m[u] = (e + u < hi && (int64_t)ga_[u] < c.n_gene_map) ? lookup(ga_[u]) : -1;
+                x[u] = xq[k][u];
+                m[u] = (e + u < hi && (int64_t)gq[k][u] < c.n_gene_map) ? lookup(gq[k][u]) : -1;
             }
+            if (bb + 128 * NB < hi) load(bb + 128 * NB, gq[k], xq[k]);
             f(m, x);
-            if (more) {
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    ga_[u] = gb_[u];
-                    xa_[u] = xb_[u];
-                }
-            }
         }
     }
 }
