@@ -193,6 +193,81 @@ struct TcArgs {
     int *err;
 };
 
+// Bounded mbarrier wait made by lane 0 and broadcast, so the calling warp
+// stays converged (the .sync.aligned tcgen05 instructions need the whole warp).
+__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
+    int got = 0;
+    if ((threadIdx.x & 31) == 0) got = mbar_wait(bar, parity, err, code) ? 1 : 0;
+    return __shfl_sync(0xffffffffu, got, 0) != 0;
+}
+
+// Epilogue warps (2 .. 9): fold each period's FP32 accumulator into FP64
+// registers, then update block (bi, bj) of G through shared memory (the
+// operand ring, idle once the last accumulator has been seen).
+__device__ __forceinline__ void tc_epilogue(const TcArgs &a, int bi, int bj, uint32_t tmem, uint8_t *ring,
+                                            uint64_t *acc_full, uint64_t *acc_empty, int n_periods, int *epi_ok_sh) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int &epi_ok = *epi_ok_sh;
+    auto warp_wait = [&](uint64_t *bar, uint32_t parity, int code) -> bool {
+        return ::crest::warp_wait(bar, parity, a.err, code);
+    };
+    const int q = warp & 3;              // TMEM lane quadrant this warp may access
+    const int h = (warp - 2) >> 2;       // column group: 64 h .. 64 h + 63
+    const int row = q * 32 + lane;
+    double acc[64];                      // FP64 sums of the periods
+#pragma unroll
+    for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+    bool ok = true;
+    for (int p = 0; p < n_periods; ++p) {
+        const int buf = p % kAccBufs;
+        if (!warp_wait(&acc_full[buf], (p / kAccBufs) & 1, 4)) {
+            ok = false;
+            break;
+        }
+        tc_fence_after();
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * kTile + h * 64);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {  // 16 columns at a time keeps the register footprint down
+            float v[16];
+            tmem_ld16(taddr + 16 * g, v);
+            tmem_wait_ld();
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[16 * g + j] += (double)v[j];
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[buf]);  // accumulator read out
+    }
+    // Stage the FP64 block in the operand ring (idle once the last
+    // accumulator has been seen: every MMA has read its operands), then
+    // update G row by row with coalesced accesses.
+    double *stage = reinterpret_cast<double *>(ring);
+    constexpr int kPitch = kTile + 1;
+    if (!ok) atomicExch(&epi_ok, 0);
+    if (ok) {
+#pragma unroll
+        for (int j = 0; j < 64; ++j) stage[row * kPitch + h * 64 + j] = acc[j];
+    }
+    asm volatile("bar.sync 1, %0;" ::"r"(kEpiWarps * 32) : "memory");  // the epilogue warps
+    if (epi_ok) {
+        const int e = warp - 2;
+        const double nk = (double)*a.n_kept;
+        for (int r = e; r < kTile; r += kEpiWarps) {
+            const int64_t ga = (int64_t)bi * kTile + r;
+            if (ga >= a.d) break;
+            const double ba = a.bias ? a.bias[ga] : 0.0, ca = a.colsum[ga];
+            double *grow = a.G + ga * a.d;
+            for (int cc = lane; cc < kTile; cc += 32) {
+                const int64_t gb = (int64_t)bj * kTile + cc;
+                if (gb >= a.d || gb < ga) continue;
+                double v = stage[r * kPitch + cc];
+                if (a.bias) v = v - ba * a.colsum[gb] - ca * a.bias[gb] - nk * ba * a.bias[gb];
+                grow[gb] += v;
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kThreads, 1) k_syrk_bf16x3(const __grid_constant__ CUtensorMap tmap, TcArgs a) {
     extern __shared__ uint8_t smem_dyn[];
     __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages], acc_full[kAccBufs], acc_empty[kAccBufs];
@@ -305,61 +380,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_bf16x3(const __grid_consta
         }
     } else {
         // ----------------------------------------------------------- epilogue
-        const int q = warp & 3;              // TMEM lane quadrant this warp may access
-        const int h = (warp - 2) >> 2;       // column group: 64 h .. 64 h + 63
-        const int row = q * 32 + lane;
-        double acc[64];                      // FP64 sums of the periods
-#pragma unroll
-        for (int j = 0; j < 64; ++j) acc[j] = 0.0;
-        bool ok = true;
-        for (int p = 0; p < n_periods; ++p) {
-            const int buf = p % kAccBufs;
-            if (!warp_wait(&acc_full[buf], (p / kAccBufs) & 1, 4)) {
-                ok = false;
-                break;
-            }
-            tc_fence_after();
-            const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * kTile + h * 64);
-#pragma unroll
-            for (int g = 0; g < 4; ++g) {  // 16 columns at a time keeps the register footprint down
-                float v[16];
-                tmem_ld16(taddr + 16 * g, v);
-                tmem_wait_ld();
-#pragma unroll
-                for (int j = 0; j < 16; ++j) acc[16 * g + j] += (double)v[j];
-            }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&acc_empty[buf]);  // accumulator read out
-        }
-        // Stage the FP64 block in the operand ring (idle once the last
-        // accumulator has been seen: every MMA has read its operands), then
-        // update G row by row with coalesced accesses.
-        double *stage = reinterpret_cast<double *>(ring);
-        constexpr int kPitch = kTile + 1;
-        if (!ok) atomicExch(&epi_ok, 0);
-        if (ok) {
-#pragma unroll
-            for (int j = 0; j < 64; ++j) stage[row * kPitch + h * 64 + j] = acc[j];
-        }
-        asm volatile("bar.sync 1, %0;" ::"r"(kEpiWarps * 32) : "memory");  // the epilogue warps
-        if (epi_ok) {
-            const int e = warp - 2;
-            const double nk = (double)*a.n_kept;
-            for (int r = e; r < kTile; r += kEpiWarps) {
-                const int64_t ga = (int64_t)bi * kTile + r;
-                if (ga >= a.d) break;
-                const double ba = a.bias ? a.bias[ga] : 0.0, ca = a.colsum[ga];
-                double *grow = a.G + ga * a.d;
-                for (int cc = lane; cc < kTile; cc += 32) {
-                    const int64_t gb = (int64_t)bj * kTile + cc;
-                    if (gb >= a.d || gb < ga) continue;
-                    double v = stage[r * kPitch + cc];
-                    if (a.bias) v = v - ba * a.colsum[gb] - ca * a.bias[gb] - nk * ba * a.bias[gb];
-                    grow[gb] += v;
-                }
-            }
-        }
+        tc_epilogue(a, bi, bj, tmem, ring, acc_full, acc_empty, n_periods, &epi_ok);
     }
     tc_fence_before();
     __syncthreads();
@@ -391,12 +412,13 @@ struct ErrFlag {
 static ErrFlag g_tc_err[64];
 
 // Device error word of the current device (0 = no bounded wait has timed out).
-// FP32 accumulation period in 64-cell stages (CREST_TC_FOLD, default 2: 128
-// cells; at 1M cells 1, 2 and 4 stages all keep the top-50 subspace within
-// 0.007 degree of the FP64 Gram, 8 stages drift past 0.01 degree).
+// FP32 accumulation period in stages of kStageCells cells (CREST_TC_FOLD,
+// default 128 cells; at 1M cells periods of 64, 128 and 256 cells all keep
+// the top-50 subspace within 0.007 degree of the FP64 Gram, 512 cells drift
+// past 0.01 degree).
 int tc_fold_stages() {
     const char *e = getenv("CREST_TC_FOLD");
-    int v = e ? atoi(e) : 2;
+    int v = e ? atoi(e) : 128 / kStageCells;
     return v < 1 ? 1 : (v > 64 ? 64 : v);
 }
 
@@ -453,9 +475,9 @@ int syrk_bf16x3_fold(const GramWork &w, int64_t m_pad, const DevScale &t, double
     a.G = gram;
     a.err = err;
     const size_t smem = 1024 + (size_t)kStages * kStageBytes;
+    prof::Scope ps("syrk_bf16x3_tcgen05", st);
     CREST_TRY(ensure_smem_attr((const void *)k_syrk_bf16x3, (size_t)smem));
     const int tiles = a.nb * (a.nb + 1) / 2;
-    prof::Scope ps("syrk_bf16x3_tcgen05", st);
     k_syrk_bf16x3<<<tiles, kThreads, smem, st>>>(map, a);
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
