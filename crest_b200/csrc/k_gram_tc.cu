@@ -411,7 +411,6 @@ struct ErrFlag {
 
 static ErrFlag g_tc_err[64];
 
-// Device error word of the current device (0 = no bounded wait has timed out).
 // FP32 accumulation period in stages of kStageCells cells (CREST_TC_FOLD,
 // default 128 cells; at 1M cells periods of 64, 128 and 256 cells all keep
 // the top-50 subspace within 0.007 degree of the FP64 Gram, 512 cells drift
@@ -422,6 +421,7 @@ int tc_fold_stages() {
     return v < 1 ? 1 : (v > 64 ? 64 : v);
 }
 
+// Device error word of the current device (0 = no bounded wait has timed out).
 int *tc_error_word() {
     int dev = 0;
     cudaGetDevice(&dev);

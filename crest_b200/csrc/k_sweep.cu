@@ -167,6 +167,12 @@ __device__ __forceinline__ void sweep_range(const DevChunk &c, const RangeIndex 
     }
 }
 
+__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
 // Cells [c0, c1) of the piece for this CTA: an even split of the spans.
 __device__ __forceinline__ void cta_cells(int64_t n_spans, int64_t &c0, int64_t &c1) {
     c0 = n_spans * (int64_t)blockIdx.x / gridDim.x;
@@ -175,19 +181,20 @@ __device__ __forceinline__ void cta_cells(int64_t n_spans, int64_t &c0, int64_t 
 
 // ------------------------------------------------------------------- QC
 // src/kernels.rs:164-195 for integral values.  Shared memory: per gene of
-// the current range the count and the 64-bit integer total as two u32
-// words (the low word's wrap-around is carried into the high word by the
-// thread whose add wrapped; every value is below 2^24, so an add wraps at
-// most once), then per-cell (t, f, n) of the CTA's cells.  Only 32-bit
-// integer shared-memory atomics are used (the fast ones on this part).
+// the current range the count and the integer total as two u32 sums, one of
+// the low and one of the high 16 bits of each value (values are below 2^24,
+// a CTA holds at most 65,536 cells, so neither sum can wrap and the total is
+// hi * 2^16 + lo exactly), then per-cell (t, f, n) of the CTA's cells.  Only
+// 32-bit integer shared-memory atomics without a return value are used (the
+// fast ones on this part); per-cell sums are integer lane sums.
 // status bit 1: a non-integral value was seen.
 __global__ void __launch_bounds__(kSweepThreads, 1)
     k_qc_sweep(DevChunk c, RangeIndex ix, const uint8_t *__restrict__ flag, uint32_t *__restrict__ gene_ncells,
                double *__restrict__ gene_total, RowOut ro, int *status) {
     extern __shared__ __align__(16) uint8_t smem[];
     const int S = 1 << ix.log2_s;
-    uint32_t *s_lo = reinterpret_cast<uint32_t *>(smem);  // [S] total, low word
-    uint32_t *s_hi = s_lo + S;                             // [S] total, high word
+    uint32_t *s_lo = reinterpret_cast<uint32_t *>(smem);  // [S] sum of the low 16 bits
+    uint32_t *s_hi = s_lo + S;                             // [S] sum of the high bits
     uint32_t *s_cnt = s_hi + S;                            // [S]
     int32_t *s_map = reinterpret_cast<int32_t *>(s_cnt + S);  // [S] gene_map of the range
     uint8_t *s_flag = reinterpret_cast<uint8_t *>(s_map + S);  // [S] flag of the mapped gene
@@ -219,32 +226,31 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
             s_flag[i] = m >= 0 ? flag[m] : 0;
         }
         __syncthreads();
-        double ts = 0.0, fs = 0.0;
+        uint64_t ts = 0, fs = 0;
         uint32_t n = 0;
         sweep_range(
             c, ix, r, c0, c1,
             [&](const Win &) {
-                ts = 0.0;
-                fs = 0.0;
+                ts = 0;
+                fs = 0;
                 n = 0;
             },
             [&](uint32_t g, float x, bool valid) {
                 const int j = (int)(g - g0);  // in [0, S) for a sorted row (any g < n_gene_map)
                 const int32_t m = valid && (int64_t)g < c.n_gene_map ? s_map[j] : -1;
                 if (m < 0 || x == 0.0f) return;
-                const double v = (double)x;
-                const bool ok = small_integer(v) && v > 0.0;
+                const bool ok = x > 0.0f && x < 16777216.0f && x == rintf(x);
                 non_integral = non_integral || !ok;
-                ts += v;
-                if (s_flag[j]) fs += v;
+                const uint32_t xi = ok ? (uint32_t)x : 0u;
+                ts += xi;
+                if (s_flag[j]) fs += xi;
                 n += 1;
                 atomicAdd(s_cnt + j, 1u);
-                const uint32_t add = ok ? (uint32_t)v : 0u;
-                const uint32_t old = atomicAdd(s_lo + j, add);
-                if (old + add < old) atomicAdd(s_hi + j, 1u);
+                atomicAdd(s_lo + j, xi & 0xffffu);
+                if (xi >> 16) atomicAdd(s_hi + j, xi >> 16);
             },
             [&](const Win &w) {
-                const double t = warp_sum(ts), f = warp_sum(fs);
+                const double t = (double)warp_sum_u64(ts), f = (double)warp_sum_u64(fs);
                 const uint32_t k = __reduce_add_sync(kFull, n);
                 if (lane == 0 && k) {  // one warp per cell: no race
                     const int64_t j = w.span - c0;
@@ -259,7 +265,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
             if (k) {
                 const int32_t m = s_map[i];  // counted entries have m >= 0
                 atomicAdd(gene_ncells + m, k);
-                atomicAdd(gene_total + m, (double)(((uint64_t)s_hi[i] << 32) | s_lo[i]));
+                atomicAdd(gene_total + m, (double)(((uint64_t)s_hi[i] << 16) + s_lo[i]));
                 s_cnt[i] = 0u;
                 s_lo[i] = 0u;
                 s_hi[i] = 0u;
@@ -359,21 +365,20 @@ __global__ void __launch_bounds__(256) k_cell_totals(DevChunk c, double *__restr
     for (int64_t i = warp; i < c.n_spans; i += n_warps) {
         int64_t lo, hi;
         span_row(c, i, lo, hi);
-        double s = 0.0;
+        uint64_t s = 0;  // exact while every kept value is an integer in [0, 2^24)
         bool ok = true;
         for_entries_x4<true>(c, lo, hi, [&](uint32_t g) { return ((s_keep[g >> 5] >> (g & 31)) & 1u) ? 0 : -1; },
                              [&](const int32_t (&m)[4], const float (&x)[4]) {
 #pragma unroll
                                  for (int u = 0; u < 4; ++u) {
                                      if (m[u] < 0) continue;
-                                     const double v = (double)x[u];
-                                     ok = ok && small_integer(v);
-                                     s += v;
+                                     ok = ok && x[u] >= 0.0f && x[u] < 16777216.0f && x[u] == rintf(x[u]);
+                                     s += (uint32_t)fminf(fmaxf(x[u], 0.0f), 16777215.0f);
                                  }
                              });
         double t;
         if (__all_sync(kFull, ok)) {
-            t = warp_sum(s);
+            t = (double)warp_sum_u64(s);
         } else {
             OrderedSum tot;
             for_entries<4, false>(c, lo, hi, [&](int32_t m, float x) { tot.add(m >= 0 ? (double)x : 0.0); });
@@ -408,7 +413,7 @@ int sweep_ctas(int64_t n_spans, int64_t cell_cap) {
 int launch_qc_sweep(const DevChunk &c, const RangeIndex &ix, const uint8_t *flag, uint32_t *gene_ncells,
                     double *gene_total, const RowOut &row, int *status, cudaStream_t st) {
     if (c.n_spans == 0) return CREST_OK;
-    const int64_t cap = ((int64_t)kMaxSmem - (int64_t)(1 << ix.log2_s) * 17) / 20;
+    const int64_t cap = std::min<int64_t>(((int64_t)kMaxSmem - (int64_t)(1 << ix.log2_s) * 17) / 20, 65536);
     const int ctas = sweep_ctas(c.n_spans, cap);
     const size_t smem = qc_sweep_smem(ix.log2_s, ceil_div(c.n_spans, ctas));
     CREST_REQUIRE(smem <= (size_t)kMaxSmem, CREST_EINVAL, "QC sweep: %zu B of shared memory", smem);
