@@ -218,13 +218,22 @@ int cell_totals(crest_matrix *m, const int32_t *gene_map, const DevChunk &proto,
     return CREST_OK;
 }
 
-__global__ void k_init_scores(const double *__restrict__ colsum, const double *__restrict__ V, int64_t d, int64_t k,
-                              double n, double *__restrict__ shift) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= k) return;
+// shift[j] = sum_a (colsum[a] / n) V[a][j] (crest/tl.py:72-76): one block per
+// component, each thread a strided partial sum, then a block reduction.
+__global__ void __launch_bounds__(256) k_init_scores(const double *__restrict__ colsum, const double *__restrict__ V,
+                                                     int64_t d, int64_t k, double n, double *__restrict__ shift) {
+    __shared__ double part[8];
+    const int64_t j = blockIdx.x;
     double s = 0.0;
-    for (int64_t a = 0; a < d; ++a) s += (colsum[a] / n) * V[a * k + j];
-    shift[j] = s;
+    for (int64_t a = threadIdx.x; a < d; a += blockDim.x) s += (colsum[a] / n) * V[a * k + j];
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += part[w];
+        shift[j] = t;
+    }
 }
 
 __global__ void k_fill_scores(const double *__restrict__ shift, int64_t n_rows, int64_t k, float *__restrict__ X) {
@@ -516,7 +525,7 @@ int crest_pca_solve(crest_pca *p, int64_t n, int64_t k) {
     EigStats es{};
     CREST_TRY(eig_topk(p->gram.as<double>(), p->colsum.as<double>(), p->d, n, k, p->vals.as<double>(),
                        p->vecs.as<double>(), p->total.as<double>(), &es, st));
-    k_init_scores<<<(unsigned)ceil_div(k, 64), 64, 0, st>>>(p->colsum.as<double>(), p->vecs.as<double>(), p->d, k,
+    k_init_scores<<<(unsigned)k, 256, 0, st>>>(p->colsum.as<double>(), p->vecs.as<double>(), p->d, k,
                                                            (double)n, p->shift.as<double>());
     CREST_CUDA_TRY(cudaGetLastError());
     p->stats.solve_ms = t.stop();

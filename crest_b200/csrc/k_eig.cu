@@ -198,8 +198,9 @@ int blas_handle(cublasHandle_t *out) {
     return CREST_OK;
 }
 
-// The filter's large products (C times a d x q block, d and K >= 512) go to
-// cuBLAS DGEMM; the epilogue's extra terms are formed first in O.
+// Products with a long inner dimension (K >= 512: the filter's C times a
+// d x q block, and the q x q Gram matrices of a d x q block) go to cuBLAS
+// DGEMM; the epilogue's extra terms are formed first in O.
 int gemm_blas(const Gemm &g, cudaStream_t st) {
     cublasHandle_t h;
     CREST_TRY(blas_handle(&h));
@@ -221,7 +222,7 @@ int gemm_blas(const Gemm &g, cudaStream_t st) {
 
 int gemm(const Gemm &g, GemmWs &w, cudaStream_t st) {
     prof::Scope ps("eig_gemm_fp64", st);
-    if (g.M >= 512 && g.K >= 512) return gemm_blas(g, st);
+    if (g.K >= 512) return gemm_blas(g, st);
     const int mt = (int)ceil_div(g.M, 64), nt = (int)ceil_div(g.N, 64);
     int ksplit = 1;
     if (g.K > 0) {
