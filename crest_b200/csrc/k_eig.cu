@@ -679,6 +679,12 @@ __global__ void k_permute_cols(const double *src, double *dst, int64_t d, const 
     dst[idx] = src[(int64_t)perm[j] * d + r];
 }
 
+// S = C - e I (d x d, col-major; S may be a copy of C made just before).
+__global__ void k_shift_diag(double *S, int64_t d, double e) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < d) S[i + i * d] -= e;
+}
+
 // Z[:, j] = (theta[j] - t) V[:, j] for j < nl (d x nl, col-major).
 __global__ void k_scale_cols(const double *V, const double *theta, double t, int64_t d, int nl, double *Z) {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -765,7 +771,7 @@ __global__ void k_tridiag(const double *ab, int L, double *T) {
 }
 
 struct EigWork {
-    DevBuf C, V, W, Y0, Y1, H, Q, vals, sorted, perm, scal, lz, lw, lab, res, rinv, fail;
+    DevBuf C, Cs, V, W, Y0, Y1, H, Q, vals, sorted, perm, scal, lz, lw, lab, res, rinv, fail;
     GemmWs g;
 };
 
@@ -827,6 +833,7 @@ int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_
     EigWork &w = ws[dev];
     const double nf = (double)n;
     CREST_TRY(w.C.ensure(sizeof(double) * (size_t)(d * d)));
+    CREST_TRY(w.Cs.ensure(sizeof(double) * (size_t)(d * d)));
     double *C = w.C.as<double>();
     {
         prof::Scope ps("eig_centre", st);
@@ -1022,21 +1029,31 @@ int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_
             m = std::max(2, std::min(m, std::min(m_cap, 60)));
             const double sigma1 = c / (top - e);
             double sigma = sigma1;
-            double *Yprev = Va, *Ycur = w.Y1.as<double>(), *Ynext = Y0;
+            double *Yprev = Va, *Ycur = w.Y1.as<double>();
             // Y1 = (sigma1/c) (C Va - e Va); Wa already holds C Va
             CREST_TRY(gemm(Gemm{D, qa, 0, C, D, 0, Va, D, Ycur, D, 0.0, Wa, sigma1 / c, Va, -sigma1 * e / c}, w.g, st));
+            // the three-term step with the shift folded into a copy of C:
+            // Y_{j+1} = (2 s'/c) (C - e I) Y_j - s s' Y_{j-1}, written over
+            // Y_{j-1} (one product with beta, no separate element-wise pass)
+            double *Cs = w.Cs.as<double>();
+            if (m >= 2) {
+                CREST_CUDA_TRY(cudaMemcpyAsync(Cs, C, sizeof(double) * (size_t)(d * d), cudaMemcpyDeviceToDevice, st));
+                k_shift_diag<<<(unsigned)ceil_div(d, 256), 256, 0, st>>>(Cs, d, e);
+                CREST_CUDA_TRY(cudaGetLastError());
+            }
             for (int j = 2; j <= m; ++j) {
                 const double sigma_next = 1.0 / (2.0 / sigma1 - sigma);
-                CREST_TRY(gemm(Gemm{D, qa, D, C, D, 0, Ycur, D, Ynext, D, 2.0 * sigma_next / c, Ycur,
-                                    -2.0 * sigma_next * e / c, Yprev, -sigma * sigma_next},
+                CREST_TRY(gemm(Gemm{D, qa, D, Cs, D, 0, Ycur, D, Yprev, D, 2.0 * sigma_next / c, Yprev,
+                                    -sigma * sigma_next, nullptr, 0.0},
                                w.g, st));
                 sigma = sigma_next;
                 double *t = Yprev;
                 Yprev = Ycur;
-                Ycur = Ynext;
-                Ynext = (t == Va) ? w.W.as<double>() + (int64_t)locked * d : t;  // Va's storage is reused below
+                Ycur = t;
             }
-            CREST_CUDA_TRY(cudaMemcpyAsync(Va, Ycur, sizeof(double) * (size_t)d * qa, cudaMemcpyDeviceToDevice, st));
+            if (Ycur != Va)
+                CREST_CUDA_TRY(
+                    cudaMemcpyAsync(Va, Ycur, sizeof(double) * (size_t)d * qa, cudaMemcpyDeviceToDevice, st));
         }
         CREST_TRY(orthonormalise(w, V, d, locked, qa, true, 1000 + it, st));
     }
