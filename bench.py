@@ -158,6 +158,12 @@ def build_inputs(args, rank: int, device: str):
     return wl, (indptr, indices, data), time.time() - t0
 
 
+def workload_label(w, n_cells: int) -> str:
+    """The workload as both arms name it in `config` (the method is in `dtype`)."""
+    return (f"{w.name}: {n_cells} cells x {w.n_genes} genes per GPU, NB counts (~{w.nnz_per_cell:.0f} nnz/cell, "
+            f"{w.n_clusters} clusters), HVG 2000, scale 10, 50 PCs")
+
+
 def preprocess(bf, allreduce=None):
     import crest_b200 as cb
     from crest_b200 import pp
@@ -229,8 +235,8 @@ def run_reference(args):
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"{w.name}: {w.n_cells} x {w.n_genes} NB counts, HVG 2000, scale 10, 50 PCs",
-                       "sample_cells": ns, "parallelism": "cpu threads"},
+            "config": {"workload": workload_label(w, args.cells or w.n_cells), "sample_cells": ns,
+                       "parallelism": "cpu threads"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"first {ns} cells of the workload (scale+PCA of the kept cells)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -445,9 +451,7 @@ def main_gpu(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "bf16x3", "data": "synthetic",
-                "config": {"workload": f"{wl.name}: {wl.n_cells} cells x {wl.n_genes} genes per GPU, NB counts "
-                                       f"(~{wl.nnz_per_cell:.0f} nnz/cell, {wl.n_clusters} clusters), HVG 2000, "
-                                       f"scale 10, 50 PCs, split-BF16 Gram",
+                "config": {"workload": workload_label(wl, wl.n_cells), "gram": "split-BF16 (bf16x3) tcgen05",
                            "cells_after_qc": n_rows, "nnz": nnz, "hvg": P["d"], "l2": "inputs (12 GB) > L2",
                            "parallelism": f"dp{ws}" if ws > 1 else "1 GPU"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
