@@ -13,7 +13,8 @@ is uploaded and X_pca is read back inside the timed region.  Under torchrun
 each rank holds its own 1M-cell shard (weak scaling); the FP64 Gram and
 column sums are all-reduced over NCCL before the replicated eigensolve.
 ``--impl reference`` times the CPU restatement of the reference's Rust path
-(threads = host cores) on a bounded sample of the same workload.
+(threads = host cores) on the same workload: the same matrix, drawn on host
+threads from the same generator, every cell in every step.
 """
 
 from __future__ import annotations
@@ -45,7 +46,6 @@ def parse():
     ap.add_argument("--impl", default="crest_b200", choices=["crest_b200", "reference"])
     ap.add_argument("--workload", default="1m")
     ap.add_argument("--cells", type=int, default=0, help="override the workload's cell count (testing)")
-    ap.add_argument("--cpu-sample", type=int, default=16384, help="cells of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     return ap.parse_args()
@@ -130,6 +130,20 @@ def ncu_traffic(kernel: str):
     return None
 
 
+def repo_libs_mapped():
+    """Shared objects of this repository mapped into the process (from /proc/self/maps)."""
+    out = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1] if len(line.split()) >= 6 else ""
+                if path.endswith(".so") and path.startswith(ROOT + os.sep):
+                    out.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(out)
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -139,23 +153,27 @@ def dist_env():
 
 # ------------------------------------------------------------------ workload
 def build_inputs(args, rank: int, device: str):
-    """Generate the rank's shard and run the (untimed) preprocessing that fixes
-    the HVG set and scale parameters: QC filters, normalize_total, log1p, seurat HVG."""
+    """Generate the rank's shard: the named workload (or its first --cells cells),
+    drawn on the GPU into page-locked host buffers ("gpu") or by the oracle's
+    host-thread generator ("cpu", the reference arm).  Both draw the same matrix."""
     from crest_b200 import synth
     w = synth.WORKLOADS[args.workload]
-    n_cells = args.cells or w.n_cells
-    wl = synth.Workload(w.name, n_cells, w.n_genes, w.n_clusters, w.dispersion, w.nnz_per_cell,
-                        w.seed + 1000 * rank, w.chunk_cells)
-    alloc = None
+    if rank:
+        w = synth.Workload(w.name, w.n_cells, w.n_genes, w.n_clusters, w.dispersion, w.nnz_per_cell,
+                           w.seed + 1000 * rank, w.chunk_cells)
+    n_cells = min(args.cells or w.n_cells, w.n_cells)
+    t0 = time.time()
     if device == "gpu":
         import torch
 
         def alloc(n, dt):
             t = torch.empty(int(n), dtype={np.uint32: torch.int32, np.float32: torch.float32}[dt], pin_memory=True)
             return t.numpy().view(dt)
-    t0 = time.time()
-    indptr, indices, data = synth.make_workload(wl, device=device, pinned_alloc=alloc)
-    return wl, (indptr, indices, data), time.time() - t0
+        arrays = synth.make_workload(w, n_cells=n_cells, pinned_alloc=alloc)
+    else:
+        from oracle import synth as osynth
+        arrays = osynth.make_workload(w, n_cells=n_cells)
+    return w, n_cells, arrays, time.time() - t0
 
 
 def workload_label(w, n_cells: int) -> str:
@@ -192,25 +210,29 @@ def pca_inputs(bf):
 
 
 # ------------------------------------------------------------------ reference arm
-def cpu_scale_pca(indptr, indices, data, n_genes, n_cells_sample, threads):
-    """scale + PCA of the oracle (the reference's Rust path restated in C, FP64 Gram,
-    LAPACK eigensolve) on the first n_cells_sample cells; returns (seconds, cells)."""
-    import oracle
+def cpu_prepare(indptr, indices, data, n_genes, threads):
+    """QC filters, normalize_total, log1p, seurat HVG and scale of the oracle (the
+    reference's CPU path restated: C kernels in its summation order + its numpy
+    host math); the untimed preprocessing before the scale + PCA step."""
     from oracle import pipeline as op
     from crest_b200 import synth
-    n = min(n_cells_sample, len(indptr) - 1)
-    ip = np.ascontiguousarray(indptr[: n + 1])
-    nnz = int(ip[-1])
-    f = op.Frame(ip, indices[:nnz], data[:nnz], n_genes, synth.gene_names(n_genes), threads=threads)
+    f = op.Frame(indptr, indices, data, n_genes, synth.gene_names(n_genes), threads=threads)
     f = op.filter_cells(f, min_genes=200)
     f = op.filter_genes(f, min_cells=3)
     op.normalize_total(f, 1e4)
     op.log1p(f)
     op.highly_variable_genes(f, n_top_genes=2000)
     op.scale(f, 10)
+    return f
+
+
+def cpu_step(f):
+    """One scale + PCA step of the oracle over every kept cell: FP64 Gram pass,
+    LAPACK eigensolve, projection pass.  Returns seconds."""
+    from oracle import pipeline as op
     t0 = time.perf_counter()
     op.pca(f, n_comps=50)
-    return time.perf_counter() - t0, f.n_obs
+    return time.perf_counter() - t0
 
 
 def run_reference(args):
@@ -219,27 +241,28 @@ def run_reference(args):
         return 0
     import oracle
     oracle.build()
-    from crest_b200 import synth
     threads = os.cpu_count() or 1
-    w = synth.WORKLOADS[args.workload]
-    ns = min(args.cpu_sample, args.cells or w.n_cells)
-    wl, (indptr, indices, data), _ = build_inputs(argparse.Namespace(**{**vars(args), "cells": ns}), 0, "cpu")
+    w, n_cells, (indptr, indices, data), gen_s = build_inputs(args, 0, "cpu")
+    t0 = time.time()
+    f = cpu_prepare(indptr, indices, data, w.n_genes, threads)
+    prep_s = time.time() - t0
     times = []
-    cells = 0
     for i in range(args.warmup + args.steps):
-        dt, cells = cpu_scale_pca(indptr, indices, data, wl.n_genes, ns, threads)
+        dt = cpu_step(f)
         if i >= args.warmup:
             times.append(dt)
     t = float(np.mean(times))
-    v = cells / t
+    v = f.n_obs / t
+    sample = (f"every cell of the workload ({f.n_obs} after QC) in every step: FP64 Gram pass, LAPACK "
+              f"eigensolve, projection pass")
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": workload_label(w, args.cells or w.n_cells), "sample_cells": ns,
-                       "parallelism": "cpu threads"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"first {ns} cells of the workload (scale+PCA of the kept cells)"},
-            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": {"workload": workload_label(w, n_cells), "cells_after_qc": f.n_obs,
+                       "parallelism": f"{threads} cpu threads"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "generate_s": gen_s, "preprocess_s": prep_s, "native_so_loaded": repo_libs_mapped()}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -262,7 +285,7 @@ def main_gpu(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         cdist.enable()  # per-gene sums and the Gram are summed over ranks
 
-    wl, (indptr, indices, data), gen_s = build_inputs(args, rank, "gpu")
+    wl, n_gen, (indptr, indices, data), gen_s = build_inputs(args, rank, "gpu")
     from crest_b200 import synth
     names = synth.gene_names(wl.n_genes)
     bf = cb.BioFrame.from_csr(indptr, indices, data, wl.n_genes, var=pd.DataFrame({"gene_name": names}))
@@ -385,6 +408,9 @@ def main_gpu(args):
     if "project_csr" in table:
         n_l, tot, mx = table["project_csr"]
         hbm["project_csr"] = (bytes_pass + n_rows * k * 4 * 2) / (tot / n_l / 1e3) / 1e9
+    if "extract_csr" in table:  # one CSR read per step; HVG entries and per-cell records written
+        n_l, tot, mx = table["extract_csr"]
+        hbm["extract_csr"] = bytes_pass / (tot / n_l / 1e3) / 1e9
     extra["hbm_gbs"] = hbm
     extra["hbm_frac"] = {kk: v / peaks["hbm_gbs"] for kk, v in hbm.items()}
 
@@ -438,20 +464,24 @@ def main_gpu(args):
                "d2h_bytes_per_step": int(Xh.nbytes), "ms_per_step": te * 1e3}
 
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        # the oracle (the reference's CPU path restated) on this box's host
+        # cores: one scale + PCA step over every cell of the same matrix
         import oracle
         oracle.build()
         threads = os.cpu_count() or 1
-        dt, cells = cpu_scale_pca(indptr, indices, data, wl.n_genes, args.cpu_sample, threads)
-        cpu = {"value": cells / dt, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"scale+PCA of the first {args.cpu_sample} cells (after QC/HVG) with the C port of "
-                         f"the reference's Rust path, FP64 Gram + LAPACK eigensolve"}
+        f = cpu_prepare(indptr, indices, data, wl.n_genes, threads)
+        dt = cpu_step(f)
+        cpu = {"value": f.n_obs / dt, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"one scale+PCA step over all {f.n_obs} kept cells of this workload (FP64 Gram, "
+                         f"LAPACK eigensolve, projection), the C port of the reference's Rust path"}
+        del f
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "bf16x3", "data": "synthetic",
-                "config": {"workload": workload_label(wl, wl.n_cells), "gram": "split-BF16 (bf16x3) tcgen05",
+                "config": {"workload": workload_label(wl, n_gen), "gram": "split-BF16 (bf16x3) tcgen05",
                            "cells_after_qc": n_rows, "nnz": nnz, "hvg": P["d"], "l2": "inputs (12 GB) > L2",
                            "parallelism": f"dp{ws}" if ws > 1 else "1 GPU"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,

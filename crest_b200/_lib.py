@@ -74,13 +74,13 @@ _SIGS = {
     "crest_pca_accumulate": [P, P, P, P, D, I32, P, I64, P],
     "crest_pca_reset": [P],
     "crest_pca_accumulators": [P, P, P],
+    "crest_pca_gram": [P, P],
     "crest_pca_solve": [P, I64, I64],
     "crest_pca_results": [P, P, P, P, P],
     "crest_pca_project": [P, P, P, P, D, I32, P, I64, P, I64, P, I32],
     "crest_pca_stats_get": [P, P],
     "crest_fused_forward": [P, P, P, I64, I64, P, P, I64, P, P, D, P],
     "crest_fused_backward": [P, P, P, I64, I64, P, P, I64, P, P, D, P, P, P, P],
-    "crest_synth_cpu": [P, P, P, P, P, C.c_int],
     "crest_synth_gpu": [P, P, P, P, P],
     "crest_profile_enable": [C.c_int],
     "crest_profile_count": [],

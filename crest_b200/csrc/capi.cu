@@ -251,6 +251,24 @@ int stage_hvg_code(const DevChunk &dc, const int32_t *sub_map, int64_t n_vars, i
     return launch_hvg_code(dc, sub_map, n_vars, d, buf.as<int32_t>(), st);
 }
 
+int gram_status_reset(const GramWork &w, cudaStream_t st) {
+    CREST_CUDA_TRY(cudaMemsetAsync(w.status, 0, sizeof(int), st));
+    return CREST_OK;
+}
+
+int gram_status_check(const GramWork &w, cudaStream_t st) {
+    int h = 0;
+    CREST_CUDA_TRY(cudaMemcpyAsync(&h, w.status, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CREST_CUDA_TRY(cudaStreamSynchronize(st));
+    CREST_REQUIRE(!(h & 2), CREST_EINVAL,
+                  "a cell holds the same HVG column twice (duplicate (cell, gene) entries): the dense Gram tile "
+                  "cannot represent the reference's pairwise sum; merge duplicates first");
+    CREST_REQUIRE(!(h & 4), CREST_EINVAL,
+                  "a cell with more than 512 HVG entries is not sorted by column, so duplicate entries could not "
+                  "be ruled out: sort each cell's entries by gene");
+    return CREST_OK;
+}
+
 int gram_over_chunk(const DevChunk &dc, const int32_t *code, const DevScale &ds, GramWork &w,
                            double *gram, double *colsum, cudaStream_t st) {
     for (int64_t s0 = 0; s0 < dc.n_spans; s0 += w.m_cap) {
@@ -387,11 +405,10 @@ int crest_gram_accumulate(const crest_chunk *chunk, const int32_t *sub_map, int6
     const int64_t m_cap = std::min<int64_t>(tile_cells_default(), round_up(std::max<int64_t>(s.n, 1), 64));
     CREST_TRY(x->gb.ensure(w, d, precision, m_cap));
     CREST_TRY(stage_hvg_code(dc, x->sub_map.as<int32_t>(), n_vars, d, x->code, st));
+    CREST_TRY(gram_status_reset(w, st));
     CREST_TRY(gram_over_chunk(dc, x->code.as<int32_t>(), ds, w, x->gram.as<double>(), x->colsum.as<double>(), st));
-    if (precision == CREST_GRAM_BF16X3) {
-        CREST_CUDA_TRY(cudaStreamSynchronize(st));
-        CREST_TRY(tc_check_error());
-    }
+    CREST_TRY(gram_status_check(w, st));  // the caller's gram / colsum stay untouched on error
+    if (precision == CREST_GRAM_BF16X3) CREST_TRY(tc_check_error());
     if (d) {
         CREST_CUDA_TRY(cudaMemcpyAsync(gram, x->gram.ptr, 8 * d * d, cudaMemcpyDeviceToHost, st));
         CREST_CUDA_TRY(cudaMemcpyAsync(colsum, x->colsum.ptr, 8 * d, cudaMemcpyDeviceToHost, st));

@@ -40,6 +40,15 @@ struct crest_matrix {
     crest::DevBuf totals;
     std::vector<int32_t> totals_key;
     bool totals_valid = false;
+    // compact HVG form of the last Gram pass over a device-resident matrix
+    // (read by the projection of the same maps); compact_off once its
+    // buffers could not be allocated (the passes then read the CSR)
+    crest::DevBuf cmp_code, cmp_x, cmp_n, cmp_scale, cmp_status, cls;
+    bool compact_off = false, cmp_valid = false;
+    std::vector<int64_t> cmp_cell_map;
+    std::vector<int32_t> cmp_gene_map, cmp_sub_map;
+    double cmp_target = 0.0;
+    int64_t cmp_d = -1;
 };
 
 struct crest_pca {
@@ -218,6 +227,70 @@ int cell_totals(crest_matrix *m, const int32_t *gene_map, const DevChunk &proto,
     return CREST_OK;
 }
 
+CompactHvg compact_view(crest_matrix *m) {
+    return CompactHvg{m->cmp_code.as<int32_t>(), m->cmp_x.as<float>(), m->cmp_n.as<int32_t>(),
+                      m->cmp_scale.as<double>(), m->cmp_status.as<int>()};
+}
+
+void compact_release(crest_matrix *m) {
+    for (auto *b : {&m->cmp_code, &m->cmp_x, &m->cmp_n, &m->cmp_scale, &m->cmp_status, &m->cls}) b->release();
+    m->cmp_valid = false;
+}
+
+// One read of the device-resident CSR into the compact HVG form (k_extract);
+// done = false when the matrix is streamed or the buffers do not fit, in
+// which case the Gram and projection passes read the CSR themselves.
+int compact_pass(crest_matrix *m, const DevChunk &proto, int64_t d, bool &done, cudaStream_t st) {
+    done = false;
+    m->cmp_valid = false;
+    if (m->residency != CREST_MEM_DEVICE || m->compact_off || m->n_cells == 0) return CREST_OK;
+    const size_t nnz = (size_t)std::max<int64_t>(m->nnz, 1), n = (size_t)m->n_cells;
+    if (m->cmp_code.ensure(4 * nnz) || m->cmp_x.ensure(4 * nnz) || m->cmp_n.ensure(4 * n) ||
+        m->cmp_scale.ensure(8 * n) || m->cmp_status.ensure(sizeof(int)) ||
+        m->cls.ensure(4 * gene_class_words(std::max<int64_t>(m->n_genes, 1)))) {
+        compact_release(m);
+        cudaGetLastError();
+        m->compact_off = true;
+        return CREST_OK;
+    }
+    CREST_TRY(launch_gene_class(m->code.as<int32_t>(), m->n_genes, d, m->cls.as<uint32_t>(), st));
+    CREST_CUDA_TRY(cudaMemsetAsync(m->cmp_status.ptr, 0, sizeof(int), st));
+    DevChunk c = proto;
+    c.genes = m->d_indices.as<uint32_t>();
+    c.values = m->d_data.as<float>();
+    c.first_cell = 0;
+    c.base = 0;
+    c.n_spans = m->n_cells;
+    CREST_TRY(launch_extract(c, m->cls.as<uint32_t>(), m->code.as<int32_t>(), d, compact_view(m), st));
+    done = true;
+    return CREST_OK;
+}
+
+// Duplicate-column check of the compact form: only cells whose columns were
+// not strictly increasing need the exact search.
+int compact_dup_check(crest_matrix *m, int64_t d, cudaStream_t st) {
+    int h = 0;
+    CREST_CUDA_TRY(cudaMemcpyAsync(&h, m->cmp_status.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CREST_CUDA_TRY(cudaStreamSynchronize(st));
+    if (!(h & 1)) return CREST_OK;
+    CREST_TRY(launch_dup_compact(m->d_indptr.as<int64_t>(), m->n_cells, compact_view(m), d, st));
+    CREST_CUDA_TRY(cudaMemcpyAsync(&h, m->cmp_status.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CREST_CUDA_TRY(cudaStreamSynchronize(st));
+    CREST_REQUIRE(!(h & 2), CREST_EINVAL,
+                  "a cell holds the same HVG column twice (duplicate (cell, gene) entries): the dense Gram tile "
+                  "cannot represent the reference's pairwise sum; merge duplicates first");
+    return CREST_OK;
+}
+
+bool compact_matches(const crest_matrix *m, const int64_t *cell_map, const int32_t *gene_map, const int32_t *sub_map,
+                     int64_t n_vars, double target_sum, int64_t d) {
+    return m->cmp_valid && m->cmp_d == d && m->cmp_target == target_sum &&
+           m->cmp_sub_map.size() == (size_t)n_vars &&
+           std::equal(m->cmp_cell_map.begin(), m->cmp_cell_map.end(), cell_map) &&
+           std::equal(m->cmp_gene_map.begin(), m->cmp_gene_map.end(), gene_map) &&
+           std::equal(m->cmp_sub_map.begin(), m->cmp_sub_map.end(), sub_map);
+}
+
 // shift[j] = sum_a (colsum[a] / n) V[a][j] (crest/tl.py:72-76): one block per
 // component, each thread a strided partial sum, then a block reduction.
 __global__ void __launch_bounds__(256) k_init_scores(const double *__restrict__ colsum, const double *__restrict__ V,
@@ -330,6 +403,7 @@ int crest_matrix_free(crest_matrix *m) {
     for (auto *b : {&m->cell_map, &m->gene_map, &m->flag, &m->sub_map, &m->mean, &m->std_, &m->bias, &m->range_off,
                     &m->status, &m->totals})
         b->release();
+    compact_release(m);
     for (auto &b : m->out) b.release();
     if (m->compute) cudaStreamDestroy(m->compute);
     if (m->copy) cudaStreamDestroy(m->copy);
@@ -486,12 +560,35 @@ int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
     CREST_TRY(stage_scale(m->mean, m->std_, m->bias, scale, p->d, ds, st));
     const DevChunk proto = base_chunk(m, target_sum, log1p);
     CREST_TRY(stage_hvg_code(proto, m->sub_map.as<int32_t>(), n_vars, p->d, m->code, st));
-    CREST_TRY(for_each_piece(m, proto, p->w.m_cap, [&](const DevChunk &c) {
-        return gram_over_chunk(c, m->code.as<int32_t>(), ds, p->w, p->gram.as<double>(), p->colsum.as<double>(), st);
-    }));
+    CREST_TRY(gram_status_reset(p->w, st));
+    bool compact = false;
+    CREST_TRY(compact_pass(m, proto, p->d, compact, st));
+    if (compact) {  // Gram tiles from the compact HVG form
+        const CompactHvg ch = compact_view(m);
+        for (int64_t s0 = 0; s0 < m->n_cells; s0 += p->w.m_cap) {
+            const int64_t n = std::min(p->w.m_cap, m->n_cells - s0);
+            CREST_TRY(launch_densify_compact(m->d_indptr.as<int64_t>(), s0, n, ch, target_sum, log1p, ds, p->w, st));
+            CREST_TRY(launch_syrk_fold(p->w, n, ds, p->gram.as<double>(), p->colsum.as<double>(), st));
+        }
+    } else {
+        CREST_TRY(for_each_piece(m, proto, p->w.m_cap, [&](const DevChunk &c) {
+            return gram_over_chunk(c, m->code.as<int32_t>(), ds, p->w, p->gram.as<double>(), p->colsum.as<double>(),
+                                   st);
+        }));
+    }
     p->stats.gram_ms = t.stop();
     CREST_CUDA_TRY(cudaGetLastError());
+    if (compact) CREST_TRY(compact_dup_check(m, p->d, st));
+    CREST_TRY(gram_status_check(p->w, st));
     if (p->precision == CREST_GRAM_BF16X3) CREST_TRY(tc_check_error());
+    if (compact) {  // the projection of the same maps reads this form
+        m->cmp_cell_map.assign(cell_map, cell_map + m->n_cells);
+        m->cmp_gene_map.assign(gene_map, gene_map + m->n_genes);
+        m->cmp_sub_map.assign(sub_map, sub_map + n_vars);
+        m->cmp_target = target_sum;
+        m->cmp_d = p->d;
+        m->cmp_valid = true;
+    }
     return CREST_OK;
 }
 
@@ -508,6 +605,14 @@ int crest_pca_accumulators(crest_pca *p, double **gram_dev, double **colsum_dev)
     CREST_REQUIRE(p, CREST_EINVAL, "plan is NULL");
     if (gram_dev) *gram_dev = p->gram.as<double>();
     if (colsum_dev) *colsum_dev = p->colsum.as<double>();
+    return CREST_OK;
+}
+
+int crest_pca_gram(crest_pca *p, double *gram) {
+    CREST_REQUIRE(p && gram, CREST_EINVAL, "NULL argument");
+    CREST_TRY(bind_device(p->device));
+    CREST_CUDA_TRY(cudaDeviceSynchronize());
+    CREST_CUDA_TRY(cudaMemcpy(gram, p->gram.ptr, 8 * (size_t)(p->d * p->d), cudaMemcpyDeviceToHost));
     return CREST_OK;
 }
 
@@ -572,12 +677,18 @@ int crest_pca_project(crest_pca *p, crest_matrix *m, const int64_t *cell_map, co
         k_fill_scores<<<(unsigned)ceil_div(n_rows * p->k, 256), 256, 0, st>>>(p->shift.as<double>(), n_rows, p->k, X);
     CREST_CUDA_TRY(cudaGetLastError());
     const DevChunk proto = base_chunk(m, target_sum, log1p);
-    CREST_TRY(stage_hvg_code(proto, m->sub_map.as<int32_t>(), n_vars, p->d, m->code, st));
-    CREST_TRY(m->counter.ensure(sizeof(unsigned int)));
-    CREST_TRY(for_each_piece(m, proto, m->n_cells, [&](const DevChunk &c) {
-        return launch_project(c, m->code.as<int32_t>(), p->d, ds, p->vecs.as<double>(), (int)p->k, X, 0,
-                              m->counter.as<unsigned int>(), st);
-    }));
+    if (compact_matches(m, cell_map, gene_map, sub_map, n_vars, target_sum, p->d)) {
+        CREST_TRY(launch_project_compact(m->d_indptr.as<int64_t>(), m->n_cells, m->cell_map.as<int64_t>(),
+                                         compact_view(m), target_sum, log1p, ds, p->vecs.as<double>(), (int)p->k, X,
+                                         st));
+    } else {
+        CREST_TRY(stage_hvg_code(proto, m->sub_map.as<int32_t>(), n_vars, p->d, m->code, st));
+        CREST_TRY(m->counter.ensure(sizeof(unsigned int)));
+        CREST_TRY(for_each_piece(m, proto, m->n_cells, [&](const DevChunk &c) {
+            return launch_project(c, m->code.as<int32_t>(), p->d, ds, p->vecs.as<double>(), (int)p->k, X, 0,
+                                  m->counter.as<unsigned int>(), st);
+        }));
+    }
     if (out_mem != CREST_MEM_DEVICE && n_rows * p->k)
         CREST_CUDA_TRY(cudaMemcpyAsync(out, X, 4 * (size_t)(n_rows * p->k), cudaMemcpyDeviceToHost, st));
     p->stats.project_ms = t.stop();

@@ -14,16 +14,20 @@
 // kMaxSpans, n_gene_map and n_vars <= kMaxGenes; larger chunks are rejected
 // with CREST_EINVAL.  CSR chunks (indptr) only.
 //
-// Set-up: the first call on a device looks the array's address up with
-// cudaGetSymbolAddress (which also loads this file's device code); later
-// calls reuse the address.  That first call should come before any stream
-// capture the caller runs.
+// Set-up: every call looks the array's address up on the current device
+// with cudaGetSymbolAddress; the first call on a device also loads this
+// file's device code there, so it should come before any stream capture the
+// caller runs.  (Looking it up each time, instead of caching it, keeps the
+// address right after a device reset re-creates the context.)
 //
 // Zero state: the per-gene accumulators are cleared with cudaMemsetAsync at
 // the start of every call; everything else in the scratch is written before
 // it is read.  Calls on one device share the scratch, so overlapping calls
 // would race: all calls are serialised by one process-wide lock and each
-// returns only after its results are back on the host.
+// returns only after its results are back on the host.  The copies run on
+// the per-thread default stream with pageable host memory and end in a
+// stream synchronisation, so no call may overlap a global-mode stream
+// capture on any thread.
 #include <mutex>
 
 #include "host.cuh"
@@ -54,9 +58,7 @@ constexpr size_t kScratchBytes = kOffGeneT + align256(8 * kMaxGenes);
 
 static __device__ __align__(256) unsigned char g_qc_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_lock;                   // serialises every call (scratch and host staging)
-unsigned char *g_base[kMaxDevices];  // device address of g_qc_scratch, per device
+std::mutex g_lock;  // serialises every call (scratch and host staging)
 
 // Host-side copies of the per-span and per-gene results (guarded by g_lock).
 struct HostStage {
@@ -69,15 +71,13 @@ struct HostStage {
 };
 HostStage g_stage;
 
-// Address of the scratch on the current device; looked up on first use.
-int scratch_base(int dev, unsigned char **out) {
-    if (!g_base[dev]) {
-        void *p = nullptr;
-        CREST_CUDA_TRY(cudaGetSymbolAddress(&p, g_qc_scratch));
-        CREST_REQUIRE(p != nullptr, CREST_ECUDA, "cudaGetSymbolAddress returned NULL for the QC scratch");
-        g_base[dev] = static_cast<unsigned char *>(p);
-    }
-    *out = g_base[dev];
+// Device address of the scratch on the current device.  In host code the
+// array's name only stands for it; a kernel must be given this address.
+int scratch_base(unsigned char **out) {
+    void *p = nullptr;
+    CREST_CUDA_TRY(cudaGetSymbolAddress(&p, g_qc_scratch));
+    CREST_REQUIRE(p != nullptr, CREST_ECUDA, "cudaGetSymbolAddress returned NULL for the QC scratch");
+    *out = static_cast<unsigned char *>(p);
     return CREST_OK;
 }
 
@@ -104,12 +104,9 @@ extern "C" int crest_qc_static(const crest_chunk *chunk, const uint8_t *flag, in
                   "crest_qc_static: %lld store genes / %lld kept genes, the static scratch holds at most %lld",
                   (long long)chunk->n_gene_map, (long long)n_vars, (long long)kMaxGenes);
     CREST_TRY(require_device());
-    int dev = 0;
-    CREST_CUDA_TRY(cudaGetDevice(&dev));
-    CREST_REQUIRE(dev >= 0 && dev < kMaxDevices, CREST_ERUNTIME, "device index %d out of range", dev);
     std::lock_guard<std::mutex> lock(g_lock);
     unsigned char *b = nullptr;
-    CREST_TRY(scratch_base(dev, &b));
+    CREST_TRY(scratch_base(&b));
     cudaStream_t st = cudaStreamPerThread;
 
     // The chunk's spans are cells first_cell .. first_cell + n_spans - 1, so
@@ -164,10 +161,13 @@ extern "C" int crest_qc_static(const crest_chunk *chunk, const uint8_t *flag, in
         CREST_CUDA_TRY(cudaMemcpyAsync(h.gene_t, b + kOffGeneT, 8 * n_vars, cudaMemcpyDeviceToHost, st));
     }
     CREST_CUDA_TRY(cudaStreamSynchronize(st));
+    // every row is checked before anything is added: a failing call leaves
+    // the caller's outputs untouched
+    for (int64_t i = 0; i < n_spans; ++i)
+        CREST_REQUIRE(h.row[i] < n_rows, CREST_EINVAL, "output sizes do not match the maps");
     for (int64_t i = 0; i < n_spans; ++i) {
         const int64_t r = h.row[i];
         if (r < 0) continue;
-        CREST_REQUIRE(r < n_rows, CREST_EINVAL, "output sizes do not match the maps");
         cell_total[r] += h.t[i];
         cell_ngenes[r] += h.n[i];
         cell_flag[r] += h.f[i];

@@ -43,7 +43,7 @@ inline int64_t tile_cells_default() {
 
 // A Gram tile workspace sized for d genes.
 struct GramBufs {
-    DevBuf tile, colsum_chunk, n_kept, shift;
+    DevBuf tile, colsum_chunk, n_kept, shift, status;
     int ensure(GramWork &w, int64_t d, int precision, int64_t m_cap) {
         w.d = d;
         w.d_pad = round_up(d > 0 ? d : 1, 128);
@@ -53,12 +53,14 @@ struct GramBufs {
         CREST_TRY(colsum_chunk.ensure(sizeof(double) * (size_t)w.d_pad));
         CREST_TRY(n_kept.ensure(2 * sizeof(int64_t)));  // kept count, then the work counter
         CREST_TRY(shift.ensure(sizeof(double) * (size_t)w.d_pad));
+        CREST_TRY(status.ensure(sizeof(int)));
         w.tile = tile.ptr;
         w.colsum_chunk = colsum_chunk.as<double>();
         w.n_kept = n_kept.as<int64_t>();
         w.counter = reinterpret_cast<unsigned int *>(n_kept.as<int64_t>() + 1);
         w.part32 = nullptr;
         w.shift = shift.as<double>();
+        w.status = status.as<int>();
         return CREST_OK;
     }
 };
@@ -77,6 +79,11 @@ inline DevChunk slice(const DevChunk &c, int64_t s0, int64_t n) {
 // of cells / indptr, sorted cells, monotone indptr; gene_map values < n_vars.
 int validate_chunk(const crest_chunk *c);
 int check_maps(const crest_chunk *c, int64_t n_vars);
+
+// Zero / read back the Gram work's duplicate-entry status: CREST_EINVAL when
+// some cell holds an HVG column twice or could not be checked.
+int gram_status_reset(const GramWork &w, cudaStream_t st);
+int gram_status_check(const GramWork &w, cudaStream_t st);
 
 // code: per-gene HVG codes from launch_hvg_code
 int gram_over_chunk(const DevChunk &dc, const int32_t *code, const DevScale &ds, GramWork &w, double *gram,

@@ -1,0 +1,426 @@
+// Compact HVG form of a device-resident matrix for one scale + PCA step.
+//
+// The Gram pass (src/kernels.rs:227-309) and the projection pass (:352-371)
+// both need, per cell, the normalisation total over kept genes and the
+// cell's HVG entries in entry order; only about one stored entry in eight
+// is an HVG entry.  k_extract streams the CSR once (16-byte loads, one warp
+// per cell, a 2-bit kept/HVG class per store gene in shared memory): it adds
+// up the kept values and writes the HVG entries (column, raw value) into the
+// cell's slot of a compact array laid out like the CSR (slot of cell i =
+// [indptr[i], indptr[i+1]), filled from the front), with the entry count and
+// the normalisation factor per cell.  The densify kernel of every Gram tile
+// and the projection then read only those entries.  Everything is formed
+// again in every step; nothing is carried over between steps.
+//
+// Duplicate (cell, column) entries: the reference's pairwise loop gives
+// v1^2 + v1 v2 + v2^2 on the diagonal for two entries of one gene, which a
+// dense tile cannot represent.  k_extract checks that every cell's HVG
+// columns are strictly increasing (true for gene-sorted rows and a monotone
+// column map); when some cell is not, k_dup_compact looks for a real
+// duplicate with a per-warp bit set and the Gram pass reports an error.
+#include <cuda_bf16.h>
+
+#include "kernels.cuh"
+#include "prof.cuh"
+#include "rowwarp.cuh"
+
+namespace crest {
+
+// -------------------------------------------------------- 2-bit classes
+// cls[g >> 4] bits 2 (g & 15) .. +1: bit 0 kept gene, bit 1 HVG column.
+__global__ void k_gene_class(const int32_t *__restrict__ code, int64_t n_gene_map, int64_t d,
+                             uint32_t *__restrict__ cls) {
+    const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= ceil_div(n_gene_map, 16)) return;
+    uint32_t v = 0;
+    for (int j = 0; j < 16; ++j) {
+        const int64_t g = w * 16 + j;
+        if (g >= n_gene_map) break;
+        const int32_t m = code[g];
+        const uint32_t b = m < 0 ? 0u : (m < d ? 3u : 1u);
+        v |= b << (2 * j);
+    }
+    cls[w] = v;
+}
+
+size_t gene_class_words(int64_t n_gene_map) { return (size_t)round_up(ceil_div(n_gene_map, 16), 4); }
+
+int launch_gene_class(const int32_t *code, int64_t n_gene_map, int64_t d, uint32_t *cls, cudaStream_t st) {
+    const int64_t nw = ceil_div(n_gene_map, 16);
+    if (nw == 0) return CREST_OK;
+    k_gene_class<<<(unsigned)ceil_div(nw, 256), 256, 0, st>>>(code, n_gene_map, d, cls);
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
+}
+
+// ------------------------------------------------------------- extract
+constexpr int kExtractWarps = 8;
+
+template <int DEPTH>
+__global__ void __launch_bounds__(kExtractWarps * 32, 4) k_extract(DevChunk c, const uint32_t *__restrict__ cls,
+                                                                const int32_t *__restrict__ code, int32_t d,
+                                                                CompactHvg out) {
+    extern __shared__ __align__(16) uint32_t s_cls[];
+    const int64_t nw = ceil_div(c.n_gene_map, 16);
+    for (int64_t j = threadIdx.x; j < nw; j += blockDim.x) s_cls[j] = __ldg(cls + j);
+    __syncthreads();
+    const int lane = lane_id();
+    const int64_t warp = (int64_t)blockIdx.x * kExtractWarps + (threadIdx.x >> 5);
+    const int64_t n_warps = (int64_t)gridDim.x * kExtractWarps;
+    const bool norm = c.target_sum > 0.0;
+    // lookup: -1 dropped gene, -2 kept gene outside the HVG columns, g for an HVG column
+    auto lookup = [&](uint32_t g) -> int32_t {
+        const uint32_t b = (s_cls[g >> 4] >> (2 * (g & 15))) & 3u;
+        return b == 0u ? -1 : (b == 1u ? -2 : (int32_t)g);
+    };
+    bool ordered = true;
+    for (int64_t i = warp; i < c.n_spans; i += n_warps) {
+        int64_t lo, hi;
+        const int64_t row = span_row(c, i, lo, hi);
+        const int64_t cell = c.first_cell + i;
+        if (row < 0) {
+            if (lane == 0) out.n[cell] = -1;
+            continue;
+        }
+        int32_t *oc = out.code + lo;
+        float *ox = out.x + lo;
+        double tsum = 0.0;
+        bool integral = true;
+        int nq = 0;
+        int32_t carry = -1;
+        for_entries_x4<true, DEPTH>(c, lo, hi, lookup, [&](const int32_t (&m)[4], const float (&x)[4]) {
+            bool hv[4];
+            int32_t col[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (m[u] != -1 && norm) {
+                    integral = integral && x[u] == rintf(x[u]) && fabsf(x[u]) < 16777216.0f;
+                    tsum += (double)x[u];
+                }
+                hv[u] = m[u] >= 0;
+                col[u] = hv[u] ? __ldg(code + m[u]) : 0;
+            }
+            int cnt;
+            int pos = nq + block_rank4(hv, cnt);
+            if (cnt == 0) return;
+            order_check4(hv, col, carry, ordered);
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (hv[u]) {
+                    oc[pos] = col[u];
+                    ox[pos] = x[u];
+                    ++pos;
+                }
+            nq += cnt;
+        });
+        double scale = 1.0;
+        if (norm) {
+            double total;
+            if (__all_sync(kFull, integral)) {
+                total = warp_sum(tsum);
+            } else {  // the reference's entry-order f64 sum
+                OrderedSum ts;
+                for_entries_by<4, false>(c, lo, hi, lookup, [&](int32_t m, float x) { ts.add(m != -1 ? (double)x : 0.0); });
+                total = ts.acc;
+            }
+            scale = total > 0.0 ? c.target_sum / total : 1.0;
+        }
+        if (lane == 0) {
+            out.n[cell] = nq;
+            out.scale[cell] = scale;
+        }
+    }
+    if (!__all_sync(kFull, ordered) && lane == 0) atomicOr(out.status, 1);
+}
+
+int launch_extract(const DevChunk &c, const uint32_t *cls, const int32_t *code, int64_t d, const CompactHvg &out,
+                   cudaStream_t st) {
+    if (c.n_spans == 0) return CREST_OK;
+    CREST_REQUIRE(c.base == 0 && !c.span_cell, CREST_EINVAL, "extract needs a whole CSR matrix");
+    const size_t smem = 4 * gene_class_words(c.n_gene_map);
+    CREST_REQUIRE(smem <= (size_t)kMaxSmem, CREST_EINVAL, "too many genes for the class table");
+    CREST_TRY(ensure_smem_attr((const void *)k_extract<1>, smem));
+    int per_sm = 0;
+    CREST_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_extract<1>, kExtractWarps * 32, smem));
+    const int64_t blocks = std::min<int64_t>(ceil_div(c.n_spans, kExtractWarps), (int64_t)device_sms() * std::max(per_sm, 1));
+    prof::Scope ps("extract_csr", st);
+    k_extract<1><<<(unsigned)blocks, kExtractWarps * 32, smem, st>>>(c, cls, code, (int32_t)d, out);
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
+}
+
+// ------------------------------------------------- exact duplicate check
+// Warp per cell with a bit set of d columns in shared memory: a column met
+// twice in one cell sets bit 1 of *status.
+constexpr int kDupWarps = 8;
+
+__global__ void __launch_bounds__(kDupWarps * 32) k_dup_compact(const int64_t *__restrict__ indptr,
+                                                                int64_t n_cells, CompactHvg in, int32_t d) {
+    extern __shared__ uint32_t s_bits[];
+    const int lane = lane_id(), wid = threadIdx.x >> 5;
+    const int nw = (d + 31) >> 5;
+    uint32_t *bits = s_bits + (size_t)wid * nw;
+    const int64_t warp = (int64_t)blockIdx.x * kDupWarps + wid;
+    const int64_t n_warps = (int64_t)gridDim.x * kDupWarps;
+    bool dup = false;
+    for (int64_t i = warp; i < n_cells; i += n_warps) {
+        const int n = in.n[i];
+        if (n <= 0) continue;
+        for (int j = lane; j < nw; j += 32) bits[j] = 0u;
+        __syncwarp();
+        const int32_t *cc = in.code + indptr[i];
+        for (int e = lane; e < n; e += 32) {
+            const int32_t col = cc[e];
+            const uint32_t bit = 1u << (col & 31);
+            if (atomicOr(bits + (col >> 5), bit) & bit) dup = true;
+        }
+        __syncwarp();
+    }
+    if (__any_sync(kFull, dup) && lane == 0) atomicOr(in.status, 2);
+}
+
+int launch_dup_compact(const int64_t *indptr, int64_t n_cells, const CompactHvg &in, int64_t d, cudaStream_t st) {
+    if (n_cells == 0 || d == 0) return CREST_OK;
+    const size_t smem = sizeof(uint32_t) * (size_t)kDupWarps * (size_t)((d + 31) / 32);
+    CREST_REQUIRE(smem <= (size_t)kMaxSmem, CREST_EINVAL, "d=%lld too large for the duplicate check", (long long)d);
+    CREST_TRY(ensure_smem_attr((const void *)k_dup_compact, smem));
+    const int64_t blocks = std::min<int64_t>(ceil_div(n_cells, kDupWarps), (int64_t)device_sms() * 8);
+    k_dup_compact<<<(unsigned)blocks, kDupWarps * 32, smem, st>>>(indptr, n_cells, in, (int32_t)d);
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
+}
+
+// ------------------------------------------------------------- densify
+// Tile row i < m_pad = cell cell0 + i of the compact form (padding rows past
+// n_cells and dropped cells are rows of zeros).  The row is filled with the
+// zero-entry value of every column (the shift; zeros for dropped / padding
+// rows) with 16-byte stores, then the cell's entries are transformed and
+// stored after a warp barrier -- the tile matches the CSR densify bit for
+// bit.  The colsum of S is privatised per block in shared memory.
+constexpr int kDensifyCWarps = 16;
+
+template <int MODE> struct CElem;
+template <> struct CElem<0> { using T = double; };
+template <> struct CElem<1> { using T = float; };
+template <> struct CElem<2> { using T = __nv_bfloat16; };
+
+template <int MODE>
+__global__ void __launch_bounds__(kDensifyCWarps * 32) k_densify_compact(
+    const int64_t *__restrict__ indptr, int64_t cell0, int64_t n_cells, CompactHvg in, double target_sum, int log1p,
+    DevScale t, const double *__restrict__ shift, int64_t d, int64_t d_pad, int64_t m_pad, void *tile,
+    double *__restrict__ colsum, int64_t *n_kept) {
+    using E = typename CElem<MODE>::T;
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr bool priv = MODE != 0;
+    double *s_col = reinterpret_cast<double *>(smem);
+    E *shift_row = reinterpret_cast<E *>(smem + (priv ? sizeof(double) * (size_t)round_up(d, 2) : 0));
+    if (priv) {
+        for (int64_t j = threadIdx.x; j < d_pad; j += blockDim.x) shift_row[j] = (E)((shift && j < d) ? shift[j] : 0.0);
+        for (int64_t j = threadIdx.x; j < d; j += blockDim.x) s_col[j] = 0.0;
+    }
+    __syncthreads();
+    const int lane = lane_id();
+    const int64_t warp = (int64_t)blockIdx.x * kDensifyCWarps + (threadIdx.x >> 5);
+    const int64_t n_warps = (int64_t)gridDim.x * kDensifyCWarps;
+    const int64_t nvec = d_pad * (int64_t)sizeof(E) / 16;
+    E *hi_plane = reinterpret_cast<E *>(tile);
+    E *lo_plane = hi_plane + (size_t)m_pad * d_pad;  // BF16X3 only
+    const uint4 zero = make_uint4(0, 0, 0, 0);
+    DevChunk tc;  // only target_sum / log1p are read by transform_value
+    tc.target_sum = target_sum;
+    tc.log1p = log1p;
+    int kept_count = 0;
+    for (int64_t i = warp; i < m_pad; i += n_warps) {
+        const int64_t cell = cell0 + i;
+        const int n = i < n_cells ? in.n[cell] : -1;
+        const bool kept = n >= 0;
+        E *row = hi_plane + (size_t)i * d_pad;
+        {
+            uint4 *dst = reinterpret_cast<uint4 *>(row);
+            const uint4 *src = reinterpret_cast<const uint4 *>(shift_row);
+            for (int64_t v = lane; v < nvec; v += 32) dst[v] = (priv && kept) ? src[v] : zero;
+            if (MODE == 2) {
+                uint4 *dlo = reinterpret_cast<uint4 *>(lo_plane + (size_t)i * d_pad);
+                for (int64_t v = lane; v < nvec; v += 32) dlo[v] = zero;
+            }
+        }
+        __syncwarp();  // orders the fill before the scattered entry stores
+        if (!kept) continue;
+        kept_count += 1;
+        const double scale = in.scale[cell];
+        const int64_t base = indptr[cell];
+        E *row_lo = lo_plane + (size_t)i * d_pad;
+        for (int e = lane; e < n; e += 32) {
+            const int32_t sub = __ldcs(in.code + base + e);
+            const double s = scale_value(t, sub, transform_value(tc, scale, __ldcs(in.x + base + e)));
+            if (MODE == 0) {
+                row[sub] = s;
+            } else {
+                const double z = shift ? __dadd_rn(s, __ldg(shift + sub)) : s;
+                if (MODE == 1) {
+                    row[sub] = (E)__double2float_rn(z);
+                } else {
+                    __nv_bfloat16 h, l;
+                    split_bf16(z, h, l);
+                    row[sub] = h;
+                    row_lo[sub] = l;
+                }
+                atomicAdd(s_col + sub, s);
+            }
+        }
+    }
+    if (lane == 0 && kept_count) atomicAdd(reinterpret_cast<unsigned long long *>(n_kept), (unsigned long long)kept_count);
+    if (priv) {
+        __syncthreads();
+        for (int64_t j = threadIdx.x; j < d; j += blockDim.x)
+            if (s_col[j] != 0.0) atomicAdd(colsum + j, s_col[j]);
+    }
+}
+
+template <int MODE>
+static int densify_compact_t(const int64_t *indptr, int64_t cell0, int64_t n, const CompactHvg &in,
+                             double target_sum, int log1p, const DevScale &t, const double *shift,
+                             const GramWork &w, int64_t m_pad, cudaStream_t st) {
+    using E = typename CElem<MODE>::T;
+    const size_t smem = MODE != 0 ? sizeof(double) * (size_t)round_up(w.d, 2) + sizeof(E) * (size_t)w.d_pad : 0;
+    CREST_REQUIRE(smem <= (size_t)kMaxSmem, CREST_EINVAL, "d=%lld too large for the densify buffers", (long long)w.d);
+    CREST_TRY(ensure_smem_attr((const void *)k_densify_compact<MODE>, smem));
+    int per_sm = 0;
+    CREST_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_densify_compact<MODE>,
+                                                                 kDensifyCWarps * 32, smem));
+    const int64_t blocks =
+        std::min<int64_t>(ceil_div(m_pad, kDensifyCWarps), (int64_t)device_sms() * std::max(per_sm, 1));
+    k_densify_compact<MODE><<<(unsigned)blocks, kDensifyCWarps * 32, smem, st>>>(
+        indptr, cell0, n, in, target_sum, log1p, t, shift, w.d, w.d_pad, m_pad, w.tile, w.colsum_chunk, w.n_kept);
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
+}
+
+int launch_densify_compact(const int64_t *indptr, int64_t cell0, int64_t n, const CompactHvg &in, double target_sum,
+                           int log1p, const DevScale &t, const GramWork &w, cudaStream_t st) {
+    CREST_REQUIRE(n <= w.m_cap, CREST_EINVAL, "tile holds %lld cells, piece has %lld", (long long)w.m_cap,
+                  (long long)n);
+    const int64_t m_pad = round_up(n > 0 ? n : 1, 64);
+    CREST_CUDA_TRY(cudaMemsetAsync(w.n_kept, 0, 2 * sizeof(int64_t), st));
+    CREST_CUDA_TRY(cudaMemsetAsync(w.colsum_chunk, 0, sizeof(double) * (size_t)(w.d > 0 ? w.d : 1), st));
+    const double *shift = nullptr;
+    if (w.precision != CREST_GRAM_FP64 && t.scale) {
+        CREST_TRY(launch_tile_shift(w, t, st));
+        shift = w.shift;
+    }
+    prof::Scope ps("densify", st);
+    if (w.precision == CREST_GRAM_FP64)
+        return densify_compact_t<0>(indptr, cell0, n, in, target_sum, log1p, t, nullptr, w, m_pad, st);
+    if (w.precision == CREST_GRAM_FP32)
+        return densify_compact_t<1>(indptr, cell0, n, in, target_sum, log1p, t, shift, w, m_pad, st);
+    return densify_compact_t<2>(indptr, cell0, n, in, target_sum, log1p, t, shift, w, m_pad, st);
+}
+
+// ------------------------------------------------------------ project
+// Warp per cell: the cell's compact entries are transformed in rounds of
+// kPCStage (lanes in parallel, staged in shared memory), then added in entry
+// order into KPL f64 accumulators per lane (component lane + 32 q), the V
+// rows of U entries loaded before their ordered additions -- the same f64
+// operations in the same order as src/kernels.rs:360-369, so the scores are
+// bit-identical to the CSR projection.
+constexpr int kPCWarps = 16;
+constexpr int kPCStage = 256;
+
+template <int KPL>
+__global__ void __launch_bounds__(kPCWarps * 32) k_project_compact(const int64_t *__restrict__ indptr,
+                                                                   int64_t n_cells, const int64_t *__restrict__ cell_map,
+                                                                   CompactHvg in, double target_sum, int log1p,
+                                                                   DevScale t, const double *__restrict__ V, int k,
+                                                                   float *__restrict__ out) {
+    constexpr int U = KPL >= 2 ? 4 : 8;
+    __shared__ double s_val[kPCWarps][kPCStage];
+    __shared__ int32_t s_code[kPCWarps][kPCStage];
+    const int lane = lane_id(), wid = threadIdx.x >> 5;
+    double *q_val = s_val[wid];
+    int32_t *q_code = s_code[wid];
+    const int64_t warp = (int64_t)blockIdx.x * kPCWarps + wid;
+    const int64_t n_warps = (int64_t)gridDim.x * kPCWarps;
+    DevChunk tc;
+    tc.target_sum = target_sum;
+    tc.log1p = log1p;
+    for (int64_t i = warp; i < n_cells; i += n_warps) {
+        const int n = in.n[i];
+        if (n < 0) continue;
+        const int64_t row = cell_map[i];
+        const double scale = in.scale[i];
+        const int64_t base = indptr[i];
+        double acc[KPL];
+#pragma unroll
+        for (int q = 0; q < KPL; ++q) acc[q] = 0.0;
+        for (int r0 = 0; r0 < n; r0 += kPCStage) {
+            const int m = n - r0 < kPCStage ? n - r0 : kPCStage;
+            __syncwarp();
+            for (int e = lane; e < m; e += 32) {
+                const int32_t sub = __ldcs(in.code + base + r0 + e);
+                q_code[e] = sub;
+                q_val[e] = scale_value(t, sub, transform_value(tc, scale, __ldcs(in.x + base + r0 + e)));
+            }
+            __syncwarp();
+            int e = 0;
+            for (; e + U <= m; e += U) {
+                double vv[U][KPL];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const double *vr = V + (size_t)q_code[e + u] * k;
+#pragma unroll
+                    for (int q = 0; q < KPL; ++q) {
+                        const int j = lane + 32 * q;
+                        vv[u][q] = j < k ? __ldg(vr + j) : 0.0;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const double sv = q_val[e + u];
+#pragma unroll
+                    for (int q = 0; q < KPL; ++q) acc[q] = __dadd_rn(acc[q], __dmul_rn(sv, vv[u][q]));
+                }
+            }
+            for (; e < m; ++e) {
+                const double *vr = V + (size_t)q_code[e] * k;
+                const double sv = q_val[e];
+#pragma unroll
+                for (int q = 0; q < KPL; ++q) {
+                    const int j = lane + 32 * q;
+                    if (j < k) acc[q] = __dadd_rn(acc[q], __dmul_rn(sv, __ldg(vr + j)));
+                }
+            }
+        }
+        float *o = out + (size_t)row * k;
+#pragma unroll
+        for (int q = 0; q < KPL; ++q) {
+            const int j = lane + 32 * q;
+            if (j < k) atomicAdd(o + j, __double2float_rn(acc[q]));
+        }
+    }
+}
+
+template <int KPL>
+static int project_compact_k(const int64_t *indptr, int64_t n_cells, const int64_t *cell_map, const CompactHvg &in,
+                             double target_sum, int log1p, const DevScale &t, const double *V, int k, float *out,
+                             cudaStream_t st) {
+    int per_sm = 0;
+    CREST_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_project_compact<KPL>, kPCWarps * 32, 0));
+    const int64_t blocks = std::min<int64_t>(ceil_div(n_cells, kPCWarps), (int64_t)device_sms() * std::max(per_sm, 1));
+    k_project_compact<KPL><<<(unsigned)blocks, kPCWarps * 32, 0, st>>>(indptr, n_cells, cell_map, in, target_sum,
+                                                                       log1p, t, V, k, out);
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
+}
+
+int launch_project_compact(const int64_t *indptr, int64_t n_cells, const int64_t *cell_map, const CompactHvg &in,
+                           double target_sum, int log1p, const DevScale &t, const double *V, int k, float *out,
+                           cudaStream_t st) {
+    if (n_cells == 0 || k == 0) return CREST_OK;
+    CREST_REQUIRE(k <= 128, CREST_EINVAL, "project supports k <= 128 (got %d)", k);
+    prof::Scope ps("project_compact", st);
+    if (k <= 32) return project_compact_k<1>(indptr, n_cells, cell_map, in, target_sum, log1p, t, V, k, out, st);
+    if (k <= 64) return project_compact_k<2>(indptr, n_cells, cell_map, in, target_sum, log1p, t, V, k, out, st);
+    return project_compact_k<4>(indptr, n_cells, cell_map, in, target_sum, log1p, t, V, k, out, st);
+}
+
+}  // namespace crest

@@ -52,6 +52,12 @@ __global__ void k_tile_shift(int precision, const double *__restrict__ bias, int
     shift[j] = v;
 }
 
+int launch_tile_shift(const GramWork &w, const DevScale &t, cudaStream_t st) {
+    k_tile_shift<<<(unsigned)ceil_div(w.d_pad, 256), 256, 0, st>>>(w.precision, t.bias, w.d, w.d_pad, w.shift);
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
+}
+
 // ------------------------------------------------------------- HVG codes
 // code[g] for a store gene id g < n_gene_map: -1 when the gene is dropped,
 // sub_map[gene_map[g]] in [0, d) for an HVG column, d for another kept gene
@@ -105,8 +111,11 @@ bool codes_in_smem(int64_t n_gene_map, int64_t d, size_t other_smem) {
 // whose total needs the in-order fold, reads its entries a second time
 // (rare: such cells are the longest of a tile and would otherwise set its
 // duration).  The colsum of S (FP32 / BF16X3) is privatised per block in
-// shared memory.  Duplicate (cell, gene) entries are not supported (one of
-// them lands in the tile).
+// shared memory.  Duplicate (cell, column) entries, which a dense tile cannot
+// hold (the reference's pairwise loop adds v1^2 + v1 v2 + v2^2 for two
+// entries of one gene), are detected: a cell whose HVG columns are not
+// strictly increasing is searched for a repeated column (bit 1 of *status),
+// or flagged as unchecked when it overflowed the queue (bit 2).
 template <int MODE>  // 0 FP64 (T = S), 1 FP32 (T = S + shift), 2 BF16X3 (hi/lo of S + shift)
 struct RowElem;
 template <> struct RowElem<0> { using T = double; };
@@ -115,13 +124,6 @@ template <> struct RowElem<2> { using T = __nv_bfloat16; };
 
 constexpr int kDensifyWarps = 32;
 constexpr int kQueue = 512;
-
-// bf16 split of a tile value (hi + lo ~ z to 2^-17 relative).  hi may come
-// from a double rounding through f32: any nearby bf16 works, lo holds the rest.
-__device__ __forceinline__ void split_bf16(double z, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
-    hi = __float2bfloat16_rn(__double2float_rn(z));
-    lo = __float2bfloat16_rn(__double2float_rn(z - (double)__bfloat162float(hi)));
-}
 
 // Queued codes are int16 when the code table itself is (SMAP), else int32.
 template <int MODE, bool SMAP>
@@ -137,7 +139,8 @@ __global__ void __launch_bounds__(kDensifyWarps * 32, 1) k_densify(DevChunk c, c
                                                                    DevScale t, const double *__restrict__ shift,
                                                                    int64_t d, int64_t d_pad, int64_t m_pad,
                                                                    void *tile, double *__restrict__ colsum,
-                                                                   int64_t *n_kept, unsigned int *counter) {
+                                                                   int64_t *n_kept, unsigned int *counter,
+                                                                   int *status) {
     using E = typename RowElem<MODE>::T;
     using Q = typename std::conditional<SMAP, int16_t, int32_t>::type;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -175,8 +178,9 @@ __global__ void __launch_bounds__(kDensifyWarps * 32, 1) k_densify(DevChunk c, c
         const bool kept = r >= 0;
         // one pass: total of the kept values and the queue of HVG entries
         double tsum = 0.0;
-        bool ok = true, ovf = false;
+        bool ok = true, ovf = false, ordered = true;
         int nq = 0;
+        int32_t carry = -1;
         if (kept) {
             for_entries_x4<true, kDensifyDepth>(c, lo, hi, lookup, [&](const int32_t (&m)[4], const float (&x)[4]) {
                 bool hv[4];
@@ -191,6 +195,7 @@ __global__ void __launch_bounds__(kDensifyWarps * 32, 1) k_densify(DevChunk c, c
                 int cnt;
                 int pos = nq + block_rank4(hv, cnt);
                 if (cnt == 0) return;
+                order_check4(hv, m, carry, ordered);
                 if (nq + cnt > kQueue) {
                     ovf = true;
                     return;
@@ -219,6 +224,17 @@ __global__ void __launch_bounds__(kDensifyWarps * 32, 1) k_densify(DevChunk c, c
         __syncwarp();  // orders the fill before the scattered entry stores; queue visible
         if (!kept) continue;
         kept_count += 1;
+        if (!__all_sync(kFull, ordered)) {
+            // columns not strictly increasing: look for a repeated column
+            // among the queued entries (pairwise; such cells are rare)
+            bool dup = false;
+            if (!ovf) {
+                for (int a = lane; a < nq; a += 32)
+                    for (int b = 0; b < a; ++b) dup = dup || q_code[a] == q_code[b];
+            }
+            if (lane == 0) atomicOr(status, ovf ? 4 : 0);
+            if (__any_sync(kFull, dup) && lane == 0) atomicOr(status, 2);
+        }
         double scale = 1.0;
         if (norm) {
             double total;
@@ -276,7 +292,7 @@ static int launch_densify_k(const DevChunk &c, const int32_t *code, const DevSca
     if (blocks > cap) blocks = cap;
     k_densify<MODE, SMAP><<<(unsigned)blocks, kDensifyWarps * 32, smem, st>>>(c, code, t, shift, w.d, w.d_pad, m_pad,
                                                                                w.tile, w.colsum_chunk, w.n_kept,
-                                                                               w.counter);
+                                                                               w.counter, w.status);
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
 }
@@ -303,8 +319,7 @@ int launch_densify(const DevChunk &c, const int32_t *code, const DevScale &t, co
     CREST_CUDA_TRY(cudaMemsetAsync(w.colsum_chunk, 0, sizeof(double) * (size_t)(w.d > 0 ? w.d : 1), st));
     const double *shift = nullptr;
     if (w.precision != CREST_GRAM_FP64 && t.scale) {
-        k_tile_shift<<<(unsigned)ceil_div(w.d_pad, 256), 256, 0, st>>>(w.precision, t.bias, w.d, w.d_pad, w.shift);
-        CREST_CUDA_TRY(cudaGetLastError());
+        CREST_TRY(launch_tile_shift(w, t, st));
         shift = w.shift;
     }
     prof::Scope ps("densify", st);
@@ -391,33 +406,36 @@ __global__ void k_colsum_f64(const double *__restrict__ T, int64_t d, int64_t d_
 // ------------------------------------------------------------ FP32 SYRK
 // 128x128 upper-triangular block tiles, 256 threads, 8x8 register tile per
 // thread, K step 16 double-buffered through shared memory.  The FP32
-// register accumulators are folded into FP64 (in shared memory) every
-// kFoldSteps K steps, so FP32 rounding only ever spans kFoldSteps*16 cells;
-// the epilogue adds the FP64 tile into G with the shift correction.
-constexpr int kBM = 128, kBK = 16, kPadS = 4, kFoldSteps = 16;
-constexpr size_t kSyrkF32Smem = sizeof(float) * 2 * 2 * kBK * (kBM + kPadS) + sizeof(double) * 64 * 256;
+// register accumulators are folded into FP64 register sums every kFoldSteps
+// K steps, so an FP32 rounding chain only ever spans kFoldSteps*16 cells:
+// the error of a chain grows with its length times the partial's magnitude,
+// and at 1M cells 256-cell chains left the top-50 subspace 0.03 degree from
+// the FP64 Gram's; 32-cell chains keep it an order of magnitude closer.
+// The epilogue adds the FP64 tile into G with the shift correction.
+constexpr int kBM = 128, kBK = 16, kPadS = 4, kFoldSteps = 2;
+constexpr size_t kSyrkF32Smem = sizeof(float) * 2 * 2 * kBK * (kBM + kPadS);
 
-__global__ void __launch_bounds__(256) k_syrk_f32(const float *__restrict__ T, int64_t d, int64_t d_pad,
-                                                  int64_t m_pad, int64_t nb, const double *__restrict__ shift,
-                                                  const double *__restrict__ colsum_c,
-                                                  const int64_t *__restrict__ n_kept, double *__restrict__ G) {
+__global__ void __launch_bounds__(256, 1) k_syrk_f32(const float *__restrict__ T, int64_t d, int64_t d_pad,
+                                                     int64_t m_pad, int64_t nb, const double *__restrict__ shift,
+                                                     const double *__restrict__ colsum_c,
+                                                     const int64_t *__restrict__ n_kept, double *__restrict__ G) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float(*As)[kBK][kBM + kPadS] = reinterpret_cast<float(*)[kBK][kBM + kPadS]>(smem_raw);
     float(*Bs)[kBK][kBM + kPadS] = reinterpret_cast<float(*)[kBK][kBM + kPadS]>(smem_raw + sizeof(float) * 2 * kBK *
                                                                                                    (kBM + kPadS));
-    double *acc64 = reinterpret_cast<double *>(smem_raw + sizeof(float) * 2 * 2 * kBK * (kBM + kPadS));
     int bi, bj;
     tri_decode(blockIdx.x, nb, bi, bj);
     const int tid = threadIdx.x;
     const int tx = tid & 15, ty = tid >> 4;
     const int64_t a0 = (int64_t)bi * kBM, b0 = (int64_t)bj * kBM;
     float acc[8][8];
+    double acc64[8][8];
 #pragma unroll
     for (int p = 0; p < 8; ++p)
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             acc[p][q] = 0.0f;
-            acc64[(p * 8 + q) * 256 + tid] = 0.0;
+            acc64[p][q] = 0.0;
         }
 
     // loader: a panel is 16 cells x 128 genes = 512 float4 (rows contiguous along genes)
@@ -437,7 +455,7 @@ __global__ void __launch_bounds__(256) k_syrk_f32(const float *__restrict__ T, i
         for (int p = 0; p < 8; ++p)
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
-                acc64[(p * 8 + q) * 256 + tid] += (double)acc[p][q];
+                acc64[p][q] += (double)acc[p][q];
                 acc[p][q] = 0.0f;
             }
     };
@@ -480,7 +498,7 @@ __global__ void __launch_bounds__(256) k_syrk_f32(const float *__restrict__ T, i
         for (int q = 0; q < 8; ++q) {
             const int64_t b = b0 + (q < 4 ? tx * 4 + q : 64 + tx * 4 + q - 4);
             if (b >= d || b < a) continue;
-            double v = acc64[(p * 8 + q) * 256 + tid];
+            double v = acc64[p][q];
             if (shift) {
                 const double bb = shift[b], cb = colsum_c[b];
                 v = v - ba * cb - ca * bb - nk * ba * bb;

@@ -97,6 +97,8 @@ struct GramWork {
     float *part32;          // [d_pad * d_pad] FP32 partial (FP32 / BF16X3)
     double *shift;          // [d_pad] tile value of a zero entry: bias rounded to the tile's
                             // precision, so the (repeated) zeros are stored exactly
+    int *status;            // [1] bit 1: a cell holds one column twice; bit 2: a cell could not
+                            // be checked (unsorted, more HVG entries than the densify queue)
 };
 
 size_t gram_tile_bytes(int precision, int64_t d_pad, int64_t m_cap);
@@ -110,6 +112,35 @@ int launch_syrk_fold(const GramWork &w, int64_t m, const DevScale &t, double *gr
                      cudaStream_t st);
 // Non-zero error word of the tensor-core Gram pipeline -> CREST_ETIMEOUT (and cleared).
 int tc_check_error();
+// shift[j] = bias[j] rounded to the tile precision (the stored value of zeros).
+int launch_tile_shift(const GramWork &w, const DevScale &t, cudaStream_t st);
+
+// ------------------------------------------------- compact HVG form (k_compact.cu)
+// HVG entries of every cell of a device-resident CSR matrix, in entry order,
+// in the cell's CSR slot: entry e < n[i] of cell i is (code[indptr[i] + e],
+// x[indptr[i] + e]); n[i] = -1 for a dropped cell; scale[i] = target/total.
+struct CompactHvg {
+    int32_t *code;   // [nnz] HVG column
+    float *x;        // [nnz] raw value
+    int32_t *n;      // [n_cells]
+    double *scale;   // [n_cells]
+    int *status;     // bit 0: some cell's columns not strictly increasing; bit 1: a duplicate column
+};
+// 2-bit kept / HVG class per store gene from the code table (words of 16 genes).
+size_t gene_class_words(int64_t n_gene_map);
+int launch_gene_class(const int32_t *code, int64_t n_gene_map, int64_t d, uint32_t *cls, cudaStream_t st);
+// One read of a whole CSR matrix (c.base == 0, CSR spans) into the compact form.
+int launch_extract(const DevChunk &c, const uint32_t *cls, const int32_t *code, int64_t d, const CompactHvg &out,
+                   cudaStream_t st);
+// Exact duplicate-column check of every cell (sets bit 1 of *in.status).
+int launch_dup_compact(const int64_t *indptr, int64_t n_cells, const CompactHvg &in, int64_t d, cudaStream_t st);
+// Densify cells [cell0, cell0 + n) of the compact form into the Gram tile.
+int launch_densify_compact(const int64_t *indptr, int64_t cell0, int64_t n, const CompactHvg &in, double target_sum,
+                           int log1p, const DevScale &t, const GramWork &w, cudaStream_t st);
+// out[cell_map[i]] += scores of cell i (bit-identical to launch_project).
+int launch_project_compact(const int64_t *indptr, int64_t n_cells, const int64_t *cell_map, const CompactHvg &in,
+                           double target_sum, int log1p, const DevScale &t, const double *V, int k, float *out,
+                           cudaStream_t st);
 
 // ------------------------------------------------------------ eigensolver
 struct EigStats {

@@ -11,6 +11,8 @@
 // segments are folded lane by lane in entry order.
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 #include "log1pf_libm.h"
 
@@ -247,6 +249,40 @@ __device__ __forceinline__ double scale_value(const DevScale &t, int32_t g, floa
     if (!t.scale) return (double)x;
     const double z = __ddiv_rn(__dsub_rn((double)x, __ldg(t.mean + g)), __ldg(t.std + g));
     return __dsub_rn(clip_mv(z, t.max_value), __ldg(t.bias + g));
+}
+
+// Strictly increasing HVG columns of a cell, checked block by block of a
+// for_entries_x4 visit: lane l holds entries 4l .. 4l+3 of the block, col[u]
+// valid where sel[u].  carry = largest column seen in earlier blocks (-1).
+__device__ __forceinline__ void order_check4(const bool (&sel)[4], const int32_t (&col)[4], int32_t &carry,
+                                             bool &ok) {
+    const int lane = lane_id();
+    int32_t first = 0x7fffffff, last = -1;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+        if (sel[u]) {
+            if (col[u] <= last) ok = false;
+            if (first == 0x7fffffff) first = col[u];
+            last = col[u];
+        }
+    int32_t incl = last;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl = max(incl, t);
+    }
+    int32_t prev = __shfl_up_sync(kFull, incl, 1);
+    prev = lane == 0 ? carry : max(prev, carry);
+    if (last >= 0 && first <= prev) ok = false;
+    carry = max(carry, __shfl_sync(kFull, incl, 31));
+}
+
+// bf16 split of a Gram tile value (hi + lo ~ z to 2^-17 relative).  hi may
+// come from a double rounding through f32: any nearby bf16 works, lo holds
+// the rest.
+__device__ __forceinline__ void split_bf16(double z, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+    hi = __float2bfloat16_rn(__double2float_rn(z));
+    lo = __float2bfloat16_rn(__double2float_rn(z - (double)__bfloat162float(hi)));
 }
 
 }  // namespace crest

@@ -1,8 +1,7 @@
-// Synthetic count-matrix generator (CPU threads and GPU kernels with one
-// shared per-draw definition, synth_core.h).  Used to make the seeded inputs
-// of the tests and the benchmark; not part of the preprocessing path.
-#include <thread>
-#include <vector>
+// Synthetic count-matrix generator (GPU kernels over the per-draw definition
+// of synth_core.h, which a host-thread generator shares to draw the same
+// matrix).  Used to make the seeded inputs of the tests and the benchmark;
+// not part of the preprocessing path.
 
 #include "host.cuh"
 #include "synth_core.h"
@@ -43,57 +42,12 @@ __global__ void __launch_bounds__(256) k_synth(crest_synth p, int64_t c0, int64_
     }
 }
 
-void cpu_rows(const crest_synth &p, int64_t c0, int64_t c1, int64_t *row_nnz, const int64_t *indptr,
-              uint32_t *indices, float *data, int64_t base) {
-    const double phi = p.dispersion, r = 1.0 / phi;
-    for (int64_t c = c0; c < c1; ++c) {
-        const double lib = p.lib[c];
-        const double *pr = p.prob + (int64_t)p.labels[c] * p.n_genes;
-        int64_t at = indptr ? indptr[c] - base : 0, cnt = 0;
-        for (int64_t g = 0; g < p.n_genes; ++g) {
-            const uint32_t k = syn_count(lib * pr[g], phi, r, syn_uniform(p.seed, (uint64_t)c, (uint64_t)g));
-            if (!k) continue;
-            if (indices) {
-                indices[at] = (uint32_t)g;
-                data[at] = (float)k;
-                ++at;
-            }
-            ++cnt;
-        }
-        if (row_nnz) row_nnz[c] = cnt;
-    }
-}
-
-template <class F>
-void parallel_cells(int64_t n, int threads, F &&f) {
-    if (threads < 1) threads = 1;
-    std::vector<std::thread> th;
-    const int64_t per = (n + threads - 1) / threads;
-    for (int t = 0; t < threads; ++t) {
-        const int64_t a = t * per, b = std::min(n, a + per);
-        if (a >= b) break;
-        th.emplace_back([=, &f] { f(a, b); });
-    }
-    for (auto &x : th) x.join();
-}
-
 }  // namespace
 }  // namespace crest
 
 using namespace crest;
 
 extern "C" {
-
-/* CPU generator: pass indices == NULL to get row_nnz only; otherwise indptr
- * (n_cells + 1, from the counts) must be given and indices/data filled. */
-int crest_synth_cpu(const crest_synth *p, int64_t *row_nnz, const int64_t *indptr, uint32_t *indices, float *data,
-                    int threads) {
-    CREST_REQUIRE(p && p->prob && p->labels && p->lib && p->dispersion > 0, CREST_EINVAL, "bad synth parameters");
-    parallel_cells(p->n_cells, threads, [&](int64_t a, int64_t b) {
-        cpu_rows(*p, a, b, indices ? nullptr : row_nnz, indptr, indices, data, 0);
-    });
-    return CREST_OK;
-}
 
 /* GPU generator writing into host buffers: rows [c0, c1) with indptr
  * absolute (indptr[c0] may be non-zero; indices/data are indexed from

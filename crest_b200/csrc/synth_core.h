@@ -42,6 +42,10 @@ SYN_HD double syn_uniform(uint64_t seed, uint64_t cell, uint64_t gene) {
 /* Returns the count; r = 1/phi. */
 SYN_HD uint32_t syn_count(double mu, double phi, double r, double u) {
     if (!(mu > 0.0)) return 0u;
+    /* P(0) = (1 + phi mu)^(-1/phi) >= 1 - mu (Bernoulli's inequality), so a
+     * uniform clearly below 1 - mu draws zero without exp/log1p: the same
+     * count as the full test, at a fraction of the cost for rare genes. */
+    if (u < 1.0 - mu - 1e-12) return 0u;
     const double pm = phi * mu;
     const double p0 = exp(-r * log1p(pm));
     if (u < p0) return 0u;

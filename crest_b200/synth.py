@@ -7,8 +7,10 @@ lognormal(0, 0.5) fold changes; library sizes are lognormal(7.6, 0.45)
 times one global scale chosen so the expected number of non-zeros per cell
 hits the workload's target; counts are negative-binomial with dispersion phi
 (variance mu + phi mu^2).  Genes 0..9 are named ``MT-*`` so the mito QC path
-is exercised.  The count draws are made by ``crest_synth_cpu`` /
-``crest_synth_gpu`` (one counter-based uniform per cell and gene).
+is exercised.  The count draws are made on the GPU by ``crest_synth_gpu``
+(one counter-based uniform per cell and gene, defined once in
+``csrc/synth_core.h``; the test oracle draws the identical matrix on host
+threads from the same definition).
 """
 
 from __future__ import annotations
@@ -95,19 +97,14 @@ def _struct(p: Params) -> _lib.Synth:
                       _lib.ptr(p.prob), _lib.ptr(p.labels), _lib.ptr(p.lib))
 
 
-def generate(p: Params, device: str = "cpu", threads: int = 0, pinned_alloc=None):
-    """Draw the counts; returns (indptr i64, indices u32, data f32) with gene-sorted rows.
-
-    ``device`` "cpu" uses host threads, "gpu" the CUDA generator.  ``pinned_alloc``
-    (nbytes, dtype) -> array may supply page-locked output buffers."""
+def generate(p: Params, pinned_alloc=None):
+    """Draw the counts on the GPU; returns (indptr i64, indices u32, data f32) in
+    host memory with gene-sorted rows.  ``pinned_alloc`` (n, dtype) -> array may
+    supply page-locked output buffers."""
     n = len(p.labels)
     s = _struct(p)
     rn = np.zeros(n, np.int64)
-    threads = threads or os.cpu_count() or 1
-    if device == "gpu":
-        _lib.call("crest_synth_gpu", C.byref(s), _lib.ptr(rn), None, None, None)
-    else:
-        _lib.call("crest_synth_cpu", C.byref(s), _lib.ptr(rn), None, None, None, threads)
+    _lib.call("crest_synth_gpu", C.byref(s), _lib.ptr(rn), None, None, None)
     indptr = np.zeros(n + 1, np.int64)
     np.cumsum(rn, out=indptr[1:])
     nnz = int(indptr[-1])
@@ -117,10 +114,7 @@ def generate(p: Params, device: str = "cpu", threads: int = 0, pinned_alloc=None
     else:
         indices = np.empty(nnz, np.uint32)
         data = np.empty(nnz, np.float32)
-    if device == "gpu":
-        _lib.call("crest_synth_gpu", C.byref(s), None, _lib.ptr(indptr), _lib.ptr(indices), _lib.ptr(data))
-    else:
-        _lib.call("crest_synth_cpu", C.byref(s), None, _lib.ptr(indptr), _lib.ptr(indices), _lib.ptr(data), threads)
+    _lib.call("crest_synth_gpu", C.byref(s), None, _lib.ptr(indptr), _lib.ptr(indices), _lib.ptr(data))
     return indptr, indices, data
 
 
@@ -128,9 +122,15 @@ def gene_names(n_genes: int, n_mito: int = 10):
     return [f"MT-{i}" if i < n_mito else f"G{i}" for i in range(n_genes)]
 
 
-def make_workload(w: Workload, device: str = "cpu", n_cells: int = None, **kw):
-    """CSR arrays of a named workload (optionally only its first n_cells cells)."""
+def workload_params(w: Workload, n_cells: int = None) -> Params:
+    """Parameters of a named workload; with n_cells, those of its first n_cells cells
+    (the same cells, labels and library sizes as in the full workload)."""
     p = make_params(w.n_cells, w.n_genes, w.n_clusters, w.dispersion, w.nnz_per_cell, w.seed)
     if n_cells is not None and n_cells < w.n_cells:
         p = Params(p.prob, p.labels[:n_cells].copy(), p.lib[:n_cells].copy(), p.dispersion, p.seed)
-    return generate(p, device=device, **kw)
+    return p
+
+
+def make_workload(w: Workload, n_cells: int = None, **kw):
+    """CSR arrays of a named workload (optionally only its first n_cells cells), drawn on the GPU."""
+    return generate(workload_params(w, n_cells), **kw)

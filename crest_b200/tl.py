@@ -52,6 +52,12 @@ class PcaPlan:
         _lib.call("crest_pca_accumulators", self.handle, C.byref(g), C.byref(c))
         return g.value, c.value
 
+    def gram(self) -> np.ndarray:
+        """The FP64 Gram accumulator (d, d); its upper triangle holds the sums."""
+        g = np.zeros((self.d, self.d), np.float64)
+        _lib.call("crest_pca_gram", self.handle, _lib.ptr(g))
+        return g
+
     def solve(self, n: int, k: int):
         _lib.call("crest_pca_solve", self.handle, int(n), int(k))
         self.k = int(k)

@@ -121,10 +121,13 @@ int crest_qc(const crest_chunk *chunk, const uint8_t *flag, int64_t n_vars, doub
  * 12 MB per device), for callers that must not have a library allocate (or
  * free, with its implicit device synchronisation) device memory for them.
  * Limits: CSR chunks (indptr) only, nnz <= 2^20, cells per chunk <= 2^16,
- * n_gene_map and n_vars <= 2^16; larger chunks return CREST_EINVAL.  The
- * first call on a device looks the scratch up (cudaGetSymbolAddress) and
+ * n_gene_map and n_vars <= 2^16; larger chunks return CREST_EINVAL.  Every
+ * call looks the scratch up on the current device (cudaGetSymbolAddress);
+ * the first call on a device also loads the library's device code there and
  * should precede any stream capture.  Calls are serialised process-wide
- * (they share the scratch) and return after the results are on the host. */
+ * (they share the scratch) and return after the results are on the host;
+ * they copy through pageable host memory on the per-thread default stream,
+ * so no call may overlap a global-mode stream capture on any thread. */
 int crest_qc_static(const crest_chunk *chunk, const uint8_t *flag, int64_t n_vars, double *cell_total,
                     uint32_t *cell_ngenes, double *cell_flag, int64_t n_rows, uint32_t *gene_ncells,
                     double *gene_total);
@@ -190,6 +193,10 @@ int crest_pca_reset(crest_pca *p);
 /* Device pointers of the FP64 accumulators (gram d*d, colsum d), e.g. for
  * an all-reduce across ranks before crest_pca_solve. */
 int crest_pca_accumulators(crest_pca *p, double **gram_dev, double **colsum_dev);
+/* Copy of the FP64 Gram accumulator (d x d row-major, upper triangle
+ * meaningful) to a host buffer: the `gram` the reference's gram_accumulate
+ * leaves in the caller's array (src/py.rs:270-287). */
+int crest_pca_gram(crest_pca *p, double *gram);
 /* Centring + top-k eigensolve on the device; n = number of cells. */
 int crest_pca_solve(crest_pca *p, int64_t n, int64_t k);
 /* Results of the solve (host): variance (k), loadings (d, k), total,
@@ -251,8 +258,6 @@ typedef struct crest_synth {
     const int32_t *labels; /* [n_cells]                              */
     const double *lib;     /* [n_cells] expected total count         */
 } crest_synth;
-int crest_synth_cpu(const crest_synth *p, int64_t *row_nnz, const int64_t *indptr, uint32_t *indices, float *data,
-                    int threads);
 int crest_synth_gpu(const crest_synth *p, int64_t *row_nnz, const int64_t *indptr, uint32_t *indices, float *data);
 
 #ifdef __cplusplus

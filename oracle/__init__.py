@@ -27,6 +27,9 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "liboracle.so")
 _SRC = os.path.join(_HERE, "crest_oracle.c")
+_SYNTH_SRC = os.path.join(_HERE, "synth_cpu.c")
+# the per-draw definition shared with the product's GPU generator
+_SYNTH_HDR = os.path.join(os.path.dirname(_HERE), "crest_b200", "csrc", "synth_core.h")
 _lib = None
 
 # rayon::current_num_threads() of the emulated reference run; it only decides
@@ -36,10 +39,12 @@ DEFAULT_THREADS = int(os.environ.get("CREST_ORACLE_THREADS", os.cpu_count() or 1
 
 def build(force: bool = False) -> str:
     """Compile the C restatement into ``oracle/liboracle.so`` (gcc, no FMA contraction)."""
-    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < os.path.getmtime(_SRC):
-        cmd = ["gcc", "-O2", "-std=c11", "-ffp-contract=off", "-fPIC", "-shared", "-o", _LIB_PATH, _SRC,
-               "-lm", "-lpthread"]
+    srcs = [_SRC, _SYNTH_SRC, _SYNTH_HDR]
+    if force or not os.path.exists(_LIB_PATH) or os.path.getmtime(_LIB_PATH) < max(map(os.path.getmtime, srcs)):
+        cmd = ["gcc", "-O2", "-std=c11", "-ffp-contract=off", "-fPIC", "-shared", "-I",
+               os.path.dirname(_SYNTH_HDR), "-o", _LIB_PATH + ".tmp", _SRC, _SYNTH_SRC, "-lm", "-lpthread"]
         subprocess.run(cmd, check=True)
+        os.replace(_LIB_PATH + ".tmp", _LIB_PATH)
     return _LIB_PATH
 
 
@@ -66,6 +71,7 @@ def lib():
         L.oc_project.argtypes = [P, C.c_int, P, C.c_int, P, P, C.c_double, P, C.c_int64, P]
         L.oc_materialize.argtypes = [P, C.c_int, P, P, P, C.c_int64]
         L.oc_materialize.restype = C.c_int64
+        L.oc_synth.argtypes = [P, P, P, P, P, C.c_int]
         _lib = L
     return _lib
 

@@ -31,7 +31,8 @@ def small_counts():
     """1,500 cells x 600 genes, 5 clusters, NB counts, MT- genes (the reference's test fixture shape)."""
     from crest_b200 import synth
     p = synth.make_params(1500, 600, 5, 0.5, 150.0, seed=0)
-    indptr, indices, data = synth.generate(p, device="cpu")
+    from oracle import synth as osynth
+    indptr, indices, data = osynth.generate(p)
     return indptr, indices, data, 600, synth.gene_names(600), p.labels
 
 
@@ -40,5 +41,6 @@ def pbmc_counts():
     """The small CPU-runnable workload: 2,700 cells x 32,738 genes, 8 clusters, ~820 nnz/cell."""
     from crest_b200 import synth
     w = synth.WORKLOADS["pbmc3k_like"]
-    indptr, indices, data = synth.make_workload(w, device="cpu")
+    from oracle import synth as osynth
+    indptr, indices, data = osynth.make_workload(w)
     return indptr, indices, data, w.n_genes, synth.gene_names(w.n_genes)

@@ -10,7 +10,8 @@ from crest_b200 import synth
 
 def make_case(n=3000, d=400, k=24, max_value=10.0, seed=0):
     p = synth.make_params(n, d, 5, 0.5, 60.0, seed=seed)
-    indptr, indices, data = synth.generate(p, device="cpu")
+    from oracle import synth as osynth
+    indptr, indices, data = osynth.generate(p)
     rng = np.random.default_rng(seed + 1)
     sf = np.exp(rng.normal(0.0, 0.3, n)).astype(np.float32)
     W = np.linalg.qr(rng.standard_normal((d, k)))[0].astype(np.float32)

@@ -14,8 +14,8 @@ Everything else -- maps, chunking, QC thresholds, lazy ops, the seurat HVG
 arithmetic, the PCA epilogue -- is the reference's code.  The outputs pin the
 oracle's own restatement of that orchestration (tests/test_golden.py).
 
-Run from the repository root with the reference checked out at
-/root/reference:  python tests/golden/make_golden.py
+Run from the repository root, giving the path of a checkout of the
+reference:  python tests/golden/make_golden.py <reference checkout>
 """
 
 from __future__ import annotations
@@ -27,7 +27,7 @@ import types
 import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
-REF = os.environ.get("CREST_REFERENCE", "/root/reference")
+REF = None  # the reference checkout, from the command line
 OUT = os.path.dirname(os.path.abspath(__file__))
 THREADS = 4  # rayon thread count emulated by the oracle (fixes the per-gene sum order)
 
@@ -178,14 +178,15 @@ CASES = {
 def case_input(name):
     sys.path.insert(0, ROOT)
     from crest_b200 import synth
+    from oracle import synth as osynth
     c = CASES[name]
     if c["kind"] == "params":
         p = synth.make_params(*c["args"])
-        indptr, indices, data = synth.generate(p)
+        indptr, indices, data = osynth.generate(p)
         n_genes = c["args"][1]
     else:
         w = synth.WORKLOADS[c["name"]]
-        indptr, indices, data = synth.make_workload(w)
+        indptr, indices, data = osynth.make_workload(w)
         n_genes = w.n_genes
     return indptr, indices, data, n_genes, synth.gene_names(n_genes)
 
@@ -210,4 +211,7 @@ def main():
 
 
 if __name__ == "__main__":
+    if len(sys.argv) != 2 or not os.path.isdir(os.path.join(sys.argv[1], "crest")):
+        sys.exit("usage: python tests/golden/make_golden.py <reference checkout (holds crest/)>")
+    REF = os.path.abspath(sys.argv[1])
     main()

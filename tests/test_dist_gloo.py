@@ -20,7 +20,8 @@ N_CELLS, N_GENES, N_TOP, K = 1600, 500, 120, 10
 def data():
     from crest_b200 import synth
     p = synth.make_params(N_CELLS, N_GENES, 5, 0.5, 120.0, seed=11)
-    return synth.generate(p, device="cpu")
+    from oracle import synth as osynth
+    return osynth.generate(p)
 
 
 def run_path(indptr, indices, values, reduce_host, reduce_count):

@@ -1,0 +1,150 @@
+"""GPU parity of the device-resident scale + PCA pass (one CSR read into the
+compact HVG form, Gram tiles and projection from it) against the oracle and
+against the streamed path that reads the CSR itself; duplicate (cell, gene)
+entries rejected instead of silently changing the Gram."""
+
+import numpy as np
+import pytest
+
+import oracle
+from crest_b200 import _lib, _native, tl
+from crest_b200.core import DeviceMatrix
+
+pytestmark = pytest.mark.gpu
+
+
+def setup(small_counts, seed, d_frac=0.4):
+    indptr, indices, data, n_genes = small_counts[:4]
+    n = len(indptr) - 1
+    rng = np.random.default_rng(seed)
+    keep_c = rng.random(n) >= 0.1
+    keep_g = rng.random(n_genes) >= 0.2
+    cm = np.full(n, -1, np.int64)
+    cm[keep_c] = np.arange(keep_c.sum())
+    gm = np.full(n_genes, -1, np.int32)
+    gm[keep_g] = np.arange(keep_g.sum(), dtype=np.int32)
+    nv = int(keep_g.sum())
+    mask = rng.random(nv) < d_frac
+    d = int(mask.sum())
+    sub = np.full(nv, -1, np.int32)
+    sub[mask] = np.arange(d, dtype=np.int32)
+    st = np.zeros((nv, 5))
+    oracle.gene_stats(indices, data, cm, gm, 1e4, True, None, indptr, 0, st)
+    nk = int(keep_c.sum())
+    mean = st[:, 0] / nk
+    var = np.maximum((st[:, 1] - nk * mean * mean) / (nk - 1), 0)
+    std = np.sqrt(var)
+    std[std == 0] = 1
+    return dict(indptr=indptr, indices=indices, data=data, n_genes=n_genes, cm=cm, gm=gm, nv=nv, d=d, sub=sub,
+                mean=np.ascontiguousarray(mean[mask]), std=np.ascontiguousarray(std[mask]), nr=nk)
+
+
+def plan_gram(s, residency, precision="fp64", indices=None, data=None):
+    dm = DeviceMatrix(s["indptr"], s["indices"] if indices is None else indices,
+                      s["data"] if data is None else data, s["n_genes"], residency, chunk_cells=400)
+    scale = _lib.Scale(1, _lib.ptr(s["mean"]), _lib.ptr(s["std"]), 10.0)
+    p = tl.PcaPlan(s["d"], precision)
+    p.accumulate(dm, s["cm"], s["gm"], 1e4, True, s["sub"], s["nv"], scale)
+    return p, dm, scale
+
+
+@pytest.mark.parametrize("residency", ["device", "host"])
+def test_plan_fp64_gram_bit_exact(small_counts, residency):
+    s = setup(small_counts, 3)
+    p, dm, _ = plan_gram(s, residency)
+    G = p.gram()
+    colsum = p.results()[3]
+    Go, co = np.zeros((s["d"], s["d"])), np.zeros(s["d"])
+    oracle.gram_accumulate(s["indices"], s["data"], s["cm"], s["gm"], 1e4, True, None, s["indptr"], 0, s["sub"],
+                           Go, co, True, s["mean"], s["std"], 10.0)
+    iu = np.triu_indices(s["d"])
+    assert np.array_equal(G[iu], Go[iu])
+    assert np.array_equal(colsum, co)
+    p.close()
+    dm.close()
+
+
+def test_compact_projection_equals_csr_projection(small_counts):
+    """The same plan (same loadings) projects a device-resident matrix from the
+    compact form and a streamed one from the CSR: identical scores."""
+    s = setup(small_counts, 4)
+    p, dm, scale = plan_gram(s, "device")
+    p.solve(s["nr"], 20)
+    Xa = p.project(dm, s["cm"], s["gm"], 1e4, True, s["sub"], s["nv"], scale, s["nr"])
+    dh = DeviceMatrix(s["indptr"], s["indices"], s["data"], s["n_genes"], "host", chunk_cells=300)
+    Xb = p.project(dh, s["cm"], s["gm"], 1e4, True, s["sub"], s["nv"], scale, s["nr"])
+    assert np.array_equal(Xa, Xb)
+    # and the oracle's projection with the plan's loadings adds the same per-cell sums
+    L = p.results()[1]
+    Xo = np.zeros((s["nr"], 20), np.float32)
+    oracle.project(s["indices"], s["data"], s["cm"], s["gm"], 1e4, True, None, s["indptr"], 0, s["sub"], L, Xo,
+                   True, s["mean"], s["std"], 10.0)
+    Xz = np.zeros((s["nr"], 20), np.float32)
+    _native.project(s["indices"], s["data"], s["cm"], s["gm"], 1e4, True, None, s["indptr"], 0, s["sub"], L, Xz,
+                    True, s["mean"], s["std"], 10.0)
+    assert np.array_equal(Xz, Xo)
+    for x in (p, dm, dh):
+        x.close()
+
+
+def shuffled_rows(s, seed):
+    """The same matrix with every row's entries in a random order."""
+    rng = np.random.default_rng(seed)
+    ix, dx = s["indices"].copy(), s["data"].copy()
+    ip = s["indptr"]
+    for i in range(len(ip) - 1):
+        a, b = ip[i], ip[i + 1]
+        perm = a + rng.permutation(b - a)
+        ix[a:b], dx[a:b] = s["indices"][perm], s["data"][perm]
+    return ix, dx
+
+
+@pytest.mark.parametrize("residency", ["device", "host"])
+def test_unsorted_rows_without_duplicates_are_accepted(small_counts, residency):
+    s = setup(small_counts, 5)
+    ix, dx = shuffled_rows(s, 1)
+    p0, d0, _ = plan_gram(s, residency)
+    p1, d1, _ = plan_gram(s, residency, indices=ix, data=dx)
+    iu = np.triu_indices(s["d"])
+    # the FP64 Gram sums products in cell order: row order inside a cell only
+    # changes which column a product lands in, not the order of the sums
+    assert np.array_equal(p0.gram()[iu], p1.gram()[iu])
+    for x in (p0, d0, p1, d1):
+        x.close()
+
+
+def with_duplicate(s, sorted_rows=True):
+    """Cell 7's first HVG entry stored twice (one more entry in its row)."""
+    ip, ix, dx = s["indptr"], s["indices"], s["data"]
+    hv_store = np.where(s["gm"] >= 0)[0]
+    hv_store = hv_store[s["sub"][s["gm"][hv_store]] >= 0]
+    row = ix[ip[7]:ip[8]]
+    j = int(ip[7] + np.where(np.isin(row, hv_store))[0][0])
+    pos = j + 1 if sorted_rows else int(ip[8])  # next to the original, or at the row's end
+    ix2 = np.insert(ix, pos, ix[j])
+    dx2 = np.insert(dx, pos, dx[j])
+    ip2 = ip.copy()
+    ip2[8:] += 1
+    return ip2, ix2.astype(np.uint32), dx2.astype(np.float32)
+
+
+@pytest.mark.parametrize("residency", ["device", "host"])
+@pytest.mark.parametrize("sorted_rows", [True, False])
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+def test_duplicate_entries_are_rejected(small_counts, residency, sorted_rows, precision):
+    s = setup(small_counts, 6)
+    ip2, ix2, dx2 = with_duplicate(s, sorted_rows)
+    s2 = dict(s, indptr=ip2, indices=ix2, data=dx2)
+    with pytest.raises(ValueError, match="twice"):
+        plan_gram(s2, residency, precision)
+
+
+def test_duplicate_entries_rejected_per_chunk(small_counts):
+    s = setup(small_counts, 7)
+    ip2, ix2, dx2 = with_duplicate(s)
+    G, cs = np.full((s["d"], s["d"]), 0.5), np.full(s["d"], 0.5)
+    with pytest.raises(ValueError, match="twice"):
+        _native.gram_accumulate(ix2, dx2, s["cm"], s["gm"], 1e4, True, None, ip2, 0, s["sub"], G, cs, True,
+                                s["mean"], s["std"], 10.0, precision="fp32")
+    # the caller's accumulators are left as they were
+    assert np.all(G == 0.5) and np.all(cs == 0.5)

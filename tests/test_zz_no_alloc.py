@@ -7,6 +7,10 @@ parity tests: bit-exact for integral counts, 1e-13 relative for per-gene
 totals of non-integral values (atomic summation order)."""
 
 import ctypes as C
+import os
+import subprocess
+import sys
+import textwrap
 
 import numpy as np
 import pytest
@@ -72,3 +76,83 @@ def test_static_scratch_rejects_oversized_chunks():
     rc = _call("crest_qc_static", ch, np.zeros(nv, bool), nv, nr, o)
     assert rc == _lib.EINVAL
     assert b"static scratch holds at most" in _lib.load().crest_last_error()
+
+
+@pytest.mark.parametrize("map_len", [700, 640, 100])
+def test_static_scratch_short_cell_map(small_counts, map_len):
+    """cell_map shorter than first_cell + n_spans: cells past its end are
+    dropped (src/kernels.rs:65-68), including a chunk that starts past it."""
+    indptr, indices, data, n_genes = small_counts[:4]
+    n = len(indptr) - 1
+    cm = np.arange(map_len, dtype=np.int64)
+    gm = np.arange(n_genes, dtype=np.int32)
+    nr, nv = map_len, n_genes
+    flag = np.zeros(nv, bool)
+    a, b = _outputs(nr, nv), _outputs(nr, nv)
+    for lo, hi in ((0, 640), (640, n)):
+        p = np.ascontiguousarray(indptr[lo:hi + 1])
+        g = np.ascontiguousarray(indices[p[0]:p[-1]])
+        v = np.ascontiguousarray(data[p[0]:p[-1]])
+        ch, keep, _, _ = _native._chunk(g, v, cm, gm, 0.0, False, None, p, lo)
+        assert _call("crest_qc", ch, flag, nv, nr, a) == _lib.OK
+        assert _call("crest_qc_static", ch, flag, nv, nr, b) == _lib.OK
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    row_sums = np.bincount(np.repeat(np.arange(n), np.diff(indptr)), weights=data.astype(np.float64), minlength=n)
+    assert np.array_equal(a[0], row_sums[:map_len])
+
+
+def test_static_scratch_bad_row_leaves_outputs_untouched(small_counts):
+    indptr, indices, data, n_genes = small_counts[:4]
+    p = np.ascontiguousarray(indptr[:51])
+    g = np.ascontiguousarray(indices[:p[-1]])
+    v = np.ascontiguousarray(data[:p[-1]])
+    cm = np.arange(50, dtype=np.int64)
+    gm = np.arange(n_genes, dtype=np.int32)
+    ch, keep, _, _ = _native._chunk(g, v, cm, gm, 0.0, False, None, p, 0)
+    o = _outputs(40, n_genes)  # rows 40..49 do not fit
+    rc = _call("crest_qc_static", ch, np.zeros(n_genes, bool), n_genes, 40, o)
+    assert rc == _lib.EINVAL
+    assert all(not x.any() for x in o)
+
+
+def test_static_scratch_allocates_nothing():
+    """In a fresh process that never calls crest_qc: after the first call (which
+    loads the device code), further calls leave the device's free memory as it is."""
+    code = textwrap.dedent("""
+        import ctypes as C, sys
+        import numpy as np
+        import torch
+        sys.path.insert(0, %r)
+        from crest_b200 import _lib, _native
+        torch.cuda.init()
+        rng = np.random.default_rng(3)
+        n, ng = 900, 700
+        counts = rng.poisson(0.3, (n, ng)).astype(np.float32)
+        indptr = np.zeros(n + 1, np.int64)
+        indptr[1:] = np.cumsum((counts > 0).sum(1))
+        genes = np.nonzero(counts)[1].astype(np.uint32)
+        vals = counts[counts > 0].astype(np.float32)
+        cm = np.arange(n, dtype=np.int64)
+        gm = np.arange(ng, dtype=np.int32)
+        ch, keep, nr, nv = _native._chunk(genes, vals, cm, gm, 0.0, False, None, indptr, 0)
+        out = [np.zeros(nr), np.zeros(nr, np.uint32), np.zeros(nr), np.zeros(nv, np.uint32), np.zeros(nv)]
+        flag = np.zeros(nv, bool)
+        P = _lib.ptr
+        def call():
+            rc = _lib.load().crest_qc_static(C.byref(ch), P(flag), nv, P(out[0]), P(out[1]), P(out[2]), nr,
+                                             P(out[3]), P(out[4]))
+            assert rc == 0, rc
+        call()
+        torch.cuda.synchronize()
+        f0 = torch.cuda.mem_get_info()[0]
+        for _ in range(5):
+            call()
+        torch.cuda.synchronize()
+        f1 = torch.cuda.mem_get_info()[0]
+        assert f1 == f0, (f0, f1)
+        assert np.array_equal(out[0], 6 * counts.sum(1))
+        print("ok")
+    """) % os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stderr[-3000:]
