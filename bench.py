@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--cells", type=int, default=0, help="override the workload's cell count (testing)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-fused", action="store_true")
     return ap.parse_args()
 
 
@@ -128,6 +129,13 @@ def ncu_traffic(kernel: str):
             if len(parts) >= 2 and not line.startswith("#") and parts[0] == kernel:
                 return float(parts[1])
     return None
+
+
+def subspace_angle_deg(A, B):
+    """Largest principal angle (degrees) between the column spaces of A and B."""
+    qa, _ = np.linalg.qr(np.asarray(A, np.float64))
+    qb, _ = np.linalg.qr(np.asarray(B, np.float64))
+    return float(np.degrees(np.arccos(np.clip(np.linalg.svd(qa.T @ qb, compute_uv=False), -1, 1))).max())
 
 
 def repo_libs_mapped():
@@ -313,7 +321,7 @@ def main_gpu(args):
         plan.project(dm, P["cmap"], P["gmap"], P["target"], P["log"], P["sub"], P["n_vars"], P["scale"], n_rows,
                      device_ptr=X.data_ptr())
 
-    def timed(precision, steps, warmup, profile=False, mark=False):
+    def timed(precision, steps, warmup, profile=False, mark=False, keep_scores=False):
         plan = tl.PcaPlan(P["d"], precision)
         for _ in range(warmup):
             plan.reset()
@@ -340,23 +348,28 @@ def main_gpu(args):
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
-        per = [e0.elapsed_time(e1) / steps]
+        ms = e0.elapsed_time(e1) / steps
         table = _lib.profile_table() if profile else {}
         if profile:
             _lib.profile_enable(False)
         stats = plan.stats()
-        loadings = plan.results()[1]
+        variance, loadings, total, _ = plan.results()
         plan.close()
-        ms = float(np.mean(per))
         if dist is not None:
             mt = torch.tensor([ms], dtype=torch.float64, device="cuda")
             dist.all_reduce(mt, op=dist.ReduceOp.MAX)
             ms = float(mt.item())
-        return ms, stats, table, loadings
+        res = {"ms": ms, "stats": stats, "table": table, "loadings": loadings, "variance_ratio": variance / total,
+               "variance": variance}
+        if keep_scores:
+            res["X"] = X.cpu().numpy()
+        return res
 
+    want_parity = rank == 0 and ws == 1 and not args.no_cpu
     peaks = measured_peaks()
     with ClockSampler(local) as clk:
-        ms, stats, _, L_bf = timed("bf16x3", args.steps, args.warmup, mark=True)
+        r_bf = timed("bf16x3", args.steps, args.warmup, mark=True, keep_scores=want_parity)
+    ms, stats = r_bf["ms"], r_bf["stats"]
     clocks = clk.summary()
     value = n_rows * ws / (ms / 1e3)
 
@@ -364,26 +377,22 @@ def main_gpu(args):
     # per-kernel device times: the same K steps again with a CUDA-event scope
     # around every launch (on its stream); the scopes' host cost makes this
     # pass a little slower, so the headline value comes from the pass above
-    ms_prof, _, table, _ = timed("bf16x3", args.steps, 1, profile=True)
-    extra["ms_per_step_profiled"] = ms_prof
+    r_prof = timed("bf16x3", args.steps, 1, profile=True)
+    table = r_prof["table"]
+    extra["ms_per_step_profiled"] = r_prof["ms"]
+    r_32 = None
     if not args.no_fp32:
-        ms32, st32, tb32, L_32 = timed("fp32", max(2, args.steps // 2), 1)
-        extra["fp32_cells_per_s"] = n_rows * ws / (ms32 / 1e3)
-        extra["fp32_ms_per_step"] = ms32
-        extra["speedup_bf16x3_vs_fp32"] = ms32 / ms
+        r_32 = timed("fp32", max(2, args.steps // 2), 1, keep_scores=want_parity)
+        extra["fp32_cells_per_s"] = n_rows * ws / (r_32["ms"] / 1e3)
+        extra["fp32_ms_per_step"] = r_32["ms"]
+        extra["speedup_bf16x3_vs_fp32"] = r_32["ms"] / ms
         # the Gram phase is the only part that differs between the two forms
-        extra["speedup_gram_bf16x3_vs_fp32"] = st32["gram_ms"] / stats["gram_ms"]
-    # accuracy of the product form against the FP64 Gram of the same run
-    ms64, st64, _, L_64 = timed("fp64", 1, 0)
-    from numpy.linalg import qr, svd
-    qa, _ = qr(L_bf)
-    qb, _ = qr(L_64)
-    ang = float(np.degrees(np.arccos(np.clip(svd(qa.T @ qb, compute_uv=False), -1, 1))).max())
-    extra["max_principal_angle_deg_vs_fp64"] = ang
-    if not args.no_fp32:
-        qc_, _ = qr(L_32)
-        extra["fp32_max_principal_angle_deg_vs_fp64"] = float(
-            np.degrees(np.arccos(np.clip(svd(qc_.T @ qb, compute_uv=False), -1, 1))).max())
+        extra["speedup_gram_bf16x3_vs_fp32"] = r_32["stats"]["gram_ms"] / stats["gram_ms"]
+    # accuracy of the product and plain forms against the FP64 Gram of the same run
+    r_64 = timed("fp64", 1, 0, keep_scores=want_parity)
+    extra["max_principal_angle_deg_vs_fp64"] = subspace_angle_deg(r_bf["loadings"], r_64["loadings"])
+    if r_32 is not None:
+        extra["fp32_max_principal_angle_deg_vs_fp64"] = subspace_angle_deg(r_32["loadings"], r_64["loadings"])
 
     # memory-bound passes (HBM GB/s): QC and gene_stats over the whole CSR
     bytes_pass = nnz * 8 + (len(indptr)) * 8
@@ -405,10 +414,7 @@ def main_gpu(args):
         if kname in tb:
             n_l, tot, mx = tb[kname]
             hbm[kname] = byts / (tot / n_l / 1e3) / 1e9
-    if "project_csr" in table:
-        n_l, tot, mx = table["project_csr"]
-        hbm["project_csr"] = (bytes_pass + n_rows * k * 4 * 2) / (tot / n_l / 1e3) / 1e9
-    if "extract_csr" in table:  # one CSR read per step; HVG entries and per-cell records written
+    if "extract_csr" in table:  # one CSR read per step (the compact HVG form is written besides)
         n_l, tot, mx = table["extract_csr"]
         hbm["extract_csr"] = bytes_pass / (tot / n_l / 1e3) / 1e9
     extra["hbm_gbs"] = hbm
@@ -441,41 +447,82 @@ def main_gpu(args):
     launches = int(sum(v[0] for v in table.values()) / max(1, args.steps))
 
     # end to end through the public API with host buffers
-    e2e = None
-    if rank == 0 or ws > 1:
-        times = []
-        for i in range(2):
+    def e2e_run(residency, reps=3):
+        times, dev_bytes, Xh = [], 0, None
+        for i in range(reps + 1):
             torch.cuda.synchronize()
+            free0 = torch.cuda.mem_get_info()[0]
             t0 = time.perf_counter()
-            m = cb.core.DeviceMatrix(indptr, indices, data, wl.n_genes, "device")
+            m = cb.core.DeviceMatrix(indptr, indices, data, wl.n_genes, residency, chunk_cells=16384)
             plan = tl.PcaPlan(P["d"], "bf16x3")
             plan.accumulate(m, P["cmap"], P["gmap"], P["target"], P["log"], P["sub"], P["n_vars"], P["scale"])
             plan.solve(n_rows, k)
             Xh = plan.project(m, P["cmap"], P["gmap"], P["target"], P["log"], P["sub"], P["n_vars"], P["scale"],
                               n_rows)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            dev_bytes = max(dev_bytes, free0 - torch.cuda.mem_get_info()[0])
             plan.close()
             m.close()
-            torch.cuda.synchronize()
-            if i > 0:
-                times.append(time.perf_counter() - t0)
+            if i > 0:  # the first run is a warm-up
+                times.append(dt)
         te = float(np.mean(times))
-        h2d = nnz * 8 + len(indptr) * 8 + P["cmap"].nbytes + P["gmap"].nbytes
-        e2e = {"value": n_rows * ws / te, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-               "d2h_bytes_per_step": int(Xh.nbytes), "ms_per_step": te * 1e3}
+        passes = 1 if residency == "device" else 2  # streamed: the Gram pass and the projection read the CSR
+        h2d = passes * (nnz * 8) + len(indptr) * 8 + 2 * P["cmap"].nbytes + 2 * P["gmap"].nbytes
+        return {"value": n_rows * ws / te, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(Xh.nbytes), "ms_per_step": te * 1e3, "repeats": reps,
+                "ms_min": min(times) * 1e3, "ms_max": max(times) * 1e3, "residency": residency,
+                "device_bytes": int(dev_bytes), "h2d_gbs_effective": h2d / te / 1e9}
 
-    cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu:
+    e2e = e2e_streamed = pcie = None
+    if rank == 0 or ws > 1:
+        e2e = e2e_run("device")
+        e2e_streamed = e2e_run("host")
+        chunk_bytes = max(int(indptr[min(i + 16384, n_gen)] - indptr[i]) for i in range(0, n_gen, 16384)) * 8
+        e2e_streamed["chunk_bytes_max"] = chunk_bytes
+        e2e_streamed["model"] = ("pinned host CSR, 16,384-cell chunks, two device buffers, copies on a second "
+                                 "stream overlapped with the kernels; device memory = two chunks + the d x d "
+                                 "Gram, its second-half copy and the eigensolver workspace")
+        # H2D bandwidth of this box (pinned, one 1 GiB copy, CUDA events)
+        hb = torch.empty(1 << 30, dtype=torch.uint8, pin_memory=True)
+        db = torch.empty(1 << 30, dtype=torch.uint8, device="cuda")
+        db.copy_(hb, non_blocking=True)
+        ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ea.record()
+        for _ in range(3):
+            db.copy_(hb, non_blocking=True)
+        eb.record()
+        torch.cuda.synchronize()
+        pcie = 3 * (1 << 30) / (ea.elapsed_time(eb) / 1e3) / 1e9
+        e2e_streamed["pcie_h2d_gbs_measured"] = pcie
+        del hb, db
+
+    cpu = parity = None
+    if want_parity:
         # the oracle (the reference's CPU path restated) on this box's host
-        # cores: one scale + PCA step over every cell of the same matrix
+        # cores, on the same matrix: its preprocessing (untimed) checks the
+        # GPU's QC / HVG results; one scale + PCA step over every kept cell
+        # is the CPU baseline and the FP64 reference of the scores
         import oracle
         oracle.build()
         threads = os.cpu_count() or 1
+        from oracle import pipeline as op
+        f_raw = op.Frame(indptr, indices, data, wl.n_genes, synth.gene_names(wl.n_genes), threads=threads)
+        oobs, ovar = op.qc_metrics(f_raw)
+        gobs, gvar = pp.calculate_qc_metrics(cb.BioFrame.from_csr(indptr, indices, data, wl.n_genes,
+                                                                  var=pd.DataFrame({"gene_name": names})),
+                                             inplace=False)
         f = cpu_prepare(indptr, indices, data, wl.n_genes, threads)
         dt = cpu_step(f)
         cpu = {"value": f.n_obs / dt, "unit": UNIT, "cores": threads, "kind": "port",
                "sample": f"one scale+PCA step over all {f.n_obs} kept cells of this workload (FP64 Gram, "
                          f"LAPACK eigensolve, projection), the C port of the reference's Rust path"}
-        del f
+        parity = parity_block(bf, f, gobs, gvar, oobs, ovar, {"bf16x3": r_bf, "fp32": r_32, "fp64": r_64})
+        del f, f_raw
+
+    fused = None
+    if rank == 0 and not args.no_fused:
+        fused = fused_leg(torch, peaks)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
@@ -484,17 +531,105 @@ def main_gpu(args):
                 "config": {"workload": workload_label(wl, n_gen), "gram": "split-BF16 (bf16x3) tcgen05",
                            "cells_after_qc": n_rows, "nnz": nnz, "hvg": P["d"], "l2": "inputs (12 GB) > L2",
                            "parallelism": f"dp{ws}" if ws > 1 else "1 GPU"},
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "e2e_streamed": e2e_streamed,
+                "gpu_launches": launches, "clocks": clocks,
                 "kernels_ms_per_step": {kk: v[1] / max(1, args.steps) for kk, v in table.items()},
                 "phases_ms": {"gram": stats["gram_ms"], "solve": stats["solve_ms"], "project": stats["project_ms"],
                               "eig_iters": stats["eig_iters"]},
-                "generate_s": gen_s, "preprocess_s": prep_s}
+                "parity_vs_oracle": parity, "differentiation": fused,
+                "generate_s": gen_s, "preprocess_s": prep_s, "native_so_loaded": repo_libs_mapped()}
         line.update(extra)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def parity_block(bf, f, gobs, gvar, oobs, ovar, runs):
+    """The GPU run against the oracle on the same 1M-cell matrix: QC integers,
+    kept sets and the HVG set (bit-exact), dispersions_norm, and per Gram form
+    the principal angles / score error / variance-ratio error of the scores."""
+    from oracle import pipeline as op
+    out = {"qc_equal": all(np.array_equal(gobs[c].to_numpy(), oobs[c]) for c in
+                           ("n_genes_by_counts", "total_counts", "pct_counts_mt")) and
+           all(np.array_equal(gvar[c].to_numpy(), ovar[c]) for c in ("n_cells_by_counts", "total_counts")),
+           "kept_cells_equal": bool(np.array_equal(bf.obs["cell_id"].to_numpy(), f.cell_ids)),
+           "kept_genes_equal": bool(np.array_equal(bf.var["gene_id"].to_numpy(), f.gene_ids)),
+           "hvg_equal": bool(np.array_equal(bf.var["highly_variable"].to_numpy(),
+                                            np.asarray(f.var["highly_variable"])))}
+    dn, odn = bf.var["dispersions_norm"].to_numpy(), np.asarray(f.var["dispersions_norm"])
+    ok = ~np.isnan(odn)
+    out["dispersions_norm_max_abs_err"] = float(np.max(np.abs(dn[ok] - odn[ok]))) if ok.any() else 0.0
+    R = f.obsm["X_pca"].astype(np.float64)
+    ovr = f.uns["pca"]["variance"]
+    for name, r in runs.items():
+        if r is None or "X" not in r:
+            continue
+        X = r["X"].astype(np.float64)
+        s = np.sign((X * R).sum(0))
+        s[s == 0] = 1
+        err = np.linalg.norm(X * s - R, axis=0) / np.linalg.norm(R, axis=0)
+        v = np.asarray(ovr, np.float64)
+        gaps = np.full(len(v), np.inf)
+        gaps[:-1] = np.minimum(gaps[:-1], (v[:-1] - v[1:]) / v[:-1])
+        gaps[1:] = np.minimum(gaps[1:], (v[:-1] - v[1:]) / v[:-1])
+        sep = gaps >= 2e-3
+        out[name] = {"max_principal_angle_deg": float(op.principal_angles_deg(X, R).max()),
+                     "score_rel_err_separated_max": float(err[sep].max()) if sep.any() else None,
+                     "separated_components": int(sep.sum()),
+                     "variance_rel_err_max": float(np.max(np.abs(r["variance"] - v) / v))}
+    return out
+
+
+def fused_leg(torch, peaks):
+    """The differentiation workload (50,000 cells x 2,000 HVG genes, ~200
+    stored entries per cell, k = 50): fused forward and backward through the
+    autograd Function, CUDA events over 5 repeats after 2 warm-ups."""
+    from crest_b200 import synth
+    from crest_b200.autograd import fused_scale_project
+    n, d, k = 50_000, 2_000, 50
+    p = synth.make_params(n, d, 20, 0.2, 200.0, seed=41)
+    indptr, indices, data = synth.generate(p)
+    rng = np.random.default_rng(42)
+    sf = np.exp(rng.normal(0.0, 0.3, n)).astype(np.float32)
+    W = np.linalg.qr(rng.standard_normal((d, k)))[0].astype(np.float32)
+    cell = np.repeat(np.arange(n), np.diff(indptr))
+    lg = np.log1p(data.astype(np.float64) / sf[cell])
+    mean = np.bincount(indices, lg, d) / n
+    std = np.sqrt(np.maximum((np.bincount(indices, lg * lg, d) - n * mean * mean) / (n - 1), 0.0))
+    std[std == 0] = 1.0
+    dev = torch.device("cuda")
+    tv = torch.tensor(data, device=dev, requires_grad=True)
+    ts = torch.tensor(sf, device=dev, requires_grad=True)
+    tw = torch.tensor(W, device=dev, requires_grad=True)
+    ti, tx = torch.tensor(indptr, device=dev), torch.tensor(indices.astype(np.int32), device=dev)
+    tm, tsd = torch.tensor(mean, device=dev), torch.tensor(std, device=dev)
+    g = torch.tensor(rng.standard_normal((n, k)).astype(np.float32), device=dev)
+    fwd, bwd = [], []
+    for i in range(7):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        out = fused_scale_project(tv, ts, tw, ti, tx, tm, tsd, 10.0)
+        e[1].record()
+        out.backward(g)
+        e[2].record()
+        torch.cuda.synchronize()
+        if i >= 2:
+            fwd.append(e[0].elapsed_time(e[1]))
+            bwd.append(e[1].elapsed_time(e[2]))
+        tv.grad = ts.grad = tw.grad = None
+    nnz = int(indptr[-1])
+    # algorithmic bytes: CSR (8 B per entry + indptr), size factors, W, mean/std, scores
+    b_fwd = nnz * 8 + (n + 1) * 8 + n * 4 + d * k * 4 + d * 16 + n * k * 4
+    b_bwd = b_fwd + nnz * 4 + n * 4 + d * k * 4  # + value, size-factor and W gradients
+    f_ms, b_ms = float(np.median(fwd)), float(np.median(bwd))
+    return {"workload": f"{n} cells x {d} HVG genes, {nnz} stored entries, k={k}",
+            "forward_ms": f_ms, "backward_ms": b_ms,
+            "forward_hbm_frac": b_fwd / (f_ms / 1e3) / 1e9 / peaks["hbm_gbs"],
+            "backward_hbm_frac": b_bwd / (b_ms / 1e3) / 1e9 / peaks["hbm_gbs"],
+            "note": "backward = value/size-factor gradients, the per-entry scaled values and the "
+                    "gene-ordered W gradient (several kernels); bytes are the algorithmic minimum"}
 
 
 def main():

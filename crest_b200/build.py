@@ -55,7 +55,7 @@ def build(force: bool = False, verbose: bool = False, jobs: int = 0) -> str:
             failed.append(src)
     if failed:
         raise RuntimeError(f"nvcc failed for {failed}")
-    link = [_nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIB + ".tmp", *objs, "-lcublas", "-lpthread"]
+    link = [_nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIB + ".tmp", *objs, "-lpthread"]
     subprocess.run(link, check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB

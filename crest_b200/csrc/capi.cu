@@ -406,7 +406,9 @@ int crest_gram_accumulate(const crest_chunk *chunk, const int32_t *sub_map, int6
     CREST_TRY(x->gb.ensure(w, d, precision, m_cap));
     CREST_TRY(stage_hvg_code(dc, x->sub_map.as<int32_t>(), n_vars, d, x->code, st));
     CREST_TRY(gram_status_reset(w, st));
+    if (w.gram_aux) CREST_CUDA_TRY(cudaMemsetAsync(w.gram_aux, 0, sizeof(double) * (size_t)(d * d), st));
     CREST_TRY(gram_over_chunk(dc, x->code.as<int32_t>(), ds, w, x->gram.as<double>(), x->colsum.as<double>(), st));
+    CREST_TRY(gram_aux_fold(w, x->gram.as<double>(), st));
     CREST_TRY(gram_status_check(w, st));  // the caller's gram / colsum stay untouched on error
     if (precision == CREST_GRAM_BF16X3) CREST_TRY(tc_check_error());
     if (d) {

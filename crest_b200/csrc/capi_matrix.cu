@@ -541,6 +541,8 @@ int crest_pca_free(crest_pca *p) {
     p->gb.colsum_chunk.release();
     p->gb.n_kept.release();
     p->gb.shift.release();
+    p->gb.status.release();
+    p->gb.aux.release();
     delete p;
     return CREST_OK;
 }
@@ -576,6 +578,7 @@ int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
                                    st);
         }));
     }
+    CREST_TRY(gram_aux_fold(p->w, p->gram.as<double>(), st));
     p->stats.gram_ms = t.stop();
     CREST_CUDA_TRY(cudaGetLastError());
     if (compact) CREST_TRY(compact_dup_check(m, p->d, st));
@@ -597,6 +600,7 @@ int crest_pca_reset(crest_pca *p) {
     CREST_TRY(bind_device(p->device));
     CREST_CUDA_TRY(cudaMemset(p->gram.ptr, 0, sizeof(double) * (size_t)(p->d * p->d)));
     CREST_CUDA_TRY(cudaMemset(p->colsum.ptr, 0, sizeof(double) * (size_t)p->d));
+    if (p->w.gram_aux) CREST_CUDA_TRY(cudaMemset(p->w.gram_aux, 0, sizeof(double) * (size_t)(p->d * p->d)));
     p->k = 0;
     return CREST_OK;
 }

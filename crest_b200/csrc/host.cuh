@@ -43,10 +43,11 @@ inline int64_t tile_cells_default() {
 
 // A Gram tile workspace sized for d genes.
 struct GramBufs {
-    DevBuf tile, colsum_chunk, n_kept, shift, status;
+    DevBuf tile, colsum_chunk, n_kept, shift, status, aux;
     int ensure(GramWork &w, int64_t d, int precision, int64_t m_cap) {
         w.d = d;
-        w.d_pad = round_up(d > 0 ? d : 1, 128);
+        // the tensor-core SYRK works on 256 x 256 blocks (pairs of SMs)
+        w.d_pad = round_up(d > 0 ? d : 1, precision == CREST_GRAM_BF16X3 ? 256 : 128);
         w.m_cap = m_cap;
         w.precision = precision;
         CREST_TRY(tile.ensure(gram_tile_bytes(precision, w.d_pad, m_cap)));
@@ -61,6 +62,14 @@ struct GramBufs {
         w.part32 = nullptr;
         w.shift = shift.as<double>();
         w.status = status.as<int>();
+        w.gram_aux = nullptr;
+        if (precision == CREST_GRAM_BF16X3 && d > 0) {
+            const size_t bytes = sizeof(double) * (size_t)d * (size_t)d;
+            const bool fresh = aux.cap < bytes;
+            CREST_TRY(aux.ensure(bytes));
+            if (fresh) CREST_CUDA_TRY(cudaMemset(aux.ptr, 0, bytes));
+            w.gram_aux = aux.as<double>();
+        }
         return CREST_OK;
     }
 };

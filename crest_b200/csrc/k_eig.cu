@@ -21,12 +21,10 @@
 //    step for the weakest wanted value, bounded so the block stays well
 //    conditioned for Cholesky QR;
 //  * orthonormalisation is shifted Cholesky QR (Fukaya et al. 2020) built
-//    from split-K FP64 GEMMs, Rayleigh-Ritz uses the same Jacobi kernel on
-//    the p x p projected matrix.
+//    from split-K FP64 GEMMs (k_gemm, this file; no library GEMM), Rayleigh-
+//    Ritz uses the same Jacobi kernel on the p x p projected matrix.
 // Stops when every wanted residual ||C v - theta v|| <= tol * theta_1.
 #include <math.h>
-
-#include <cublas_v2.h>
 
 #include <algorithm>
 #include <mutex>
@@ -91,62 +89,119 @@ struct Gemm {
     int tB = 0;  // 1: B is given transposed (element (k, n) at B[n + k ldb])
 };
 
-__global__ void __launch_bounds__(256) k_gemm(Gemm g, int kchunk, double *ws) {
-    __shared__ double As[16][64 + 1];
-    __shared__ double Bs[16][64 + 1];
-    const int m0 = blockIdx.x * 64, n0 = blockIdx.y * 64;
+// 128 x 64 output tile per CTA (128 threads, 8 x 8 outputs each: rows
+// 8 tr .. 8 tr + 7, columns 8 tc .. 8 tc + 7), K in steps of 8 staged
+// through double-buffered shared memory with the next step's loads in
+// registers.  gridDim.z splits K: each slice writes its partial product to
+// ws (summed in slice order by k_gemm_reduce, so results do not depend on
+// scheduling); without a split the epilogue is applied here.
+constexpr int kGM = 128, kGN = 64, kGK = 8;
+
+__global__ void __launch_bounds__(128) k_gemm(Gemm g, int kchunk, double *ws) {
+    __shared__ __align__(16) double As[2][kGK][kGM];
+    __shared__ __align__(16) double Bs[2][kGK][kGN];
+    const int m0 = blockIdx.x * kGM, n0 = blockIdx.y * kGN;
     const int kb = blockIdx.z * kchunk, ke = min(g.K, kb + kchunk);
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    double acc[4][4] = {};
-    for (int k0 = kb; k0 < ke; k0 += 16) {
+    const int tid = threadIdx.x, tr = tid >> 3, tc = tid & 7;
+    double acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    double ra[8], rb[4];
+    // element r of this thread's share: A (m, k) and B (k, n) of the K step at k0
+    auto a_mk = [&](int r, int &mm, int &kk) {
+        const int e = tid + 128 * r;
+        if (!g.tA) {
+            mm = e & (kGM - 1);
+            kk = e >> 7;
+        } else {
+            kk = e & (kGK - 1);
+            mm = e >> 3;
+        }
+    };
+    auto b_kn = [&](int r, int &kk, int &nn) {
+        const int e = tid + 128 * r;
+        if (!g.tB) {
+            kk = e & (kGK - 1);
+            nn = e >> 3;
+        } else {
+            nn = e & (kGN - 1);
+            kk = e >> 6;
+        }
+    };
+    auto gload = [&](int k0) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            int mm, kk;
+            a_mk(r, mm, kk);
+            const int m = m0 + mm, k = k0 + kk;
+            ra[r] = (m < g.M && k < ke) ? (g.tA ? g.A[k + (int64_t)m * g.lda] : g.A[m + (int64_t)k * g.lda]) : 0.0;
+        }
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            const int idx = tid + 256 * r;
+            int kk, nn;
+            b_kn(r, kk, nn);
+            const int n = n0 + nn, k = k0 + kk;
+            rb[r] = (n < g.N && k < ke) ? (g.tB ? g.B[n + (int64_t)k * g.ldb] : g.B[k + (int64_t)n * g.ldb]) : 0.0;
+        }
+    };
+    auto sstore = [&](int buf) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
             int mm, kk;
-            if (!g.tA) {
-                mm = idx & 63;
-                kk = idx >> 6;
-            } else {
-                kk = idx & 15;
-                mm = idx >> 4;
+            a_mk(r, mm, kk);
+            As[buf][kk][mm] = ra[r];
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            int kk, nn;
+            b_kn(r, kk, nn);
+            Bs[buf][kk][nn] = rb[r];
+        }
+    };
+    int buf = 0;
+    if (kb < ke) {
+        gload(kb);
+        sstore(0);
+    }
+    __syncthreads();
+    for (int k0 = kb; k0 < ke; k0 += kGK) {
+        const bool more = k0 + kGK < ke;
+        if (more) gload(k0 + kGK);
+#pragma unroll
+        for (int kk = 0; kk < kGK; ++kk) {
+            double a[8], b[8];
+#pragma unroll
+            for (int i = 0; i < 8; i += 2) {
+                const double2 va = *reinterpret_cast<const double2 *>(&As[buf][kk][tr * 8 + i]);
+                const double2 vb = *reinterpret_cast<const double2 *>(&Bs[buf][kk][tc * 8 + i]);
+                a[i] = va.x;
+                a[i + 1] = va.y;
+                b[i] = vb.x;
+                b[i + 1] = vb.y;
             }
-            const int m = m0 + mm, k = k0 + kk;
-            double v = 0.0;
-            if (m < g.M && k < ke) v = g.tA ? g.A[k + (int64_t)m * g.lda] : g.A[m + (int64_t)k * g.lda];
-            As[kk][mm] = v;
-            const int kq = g.tB ? idx >> 6 : idx & 15, nn = g.tB ? idx & 63 : idx >> 4;
-            const int n = n0 + nn, kB = k0 + kq;
-            double bv = 0.0;
-            if (n < g.N && kB < ke) bv = g.tB ? g.B[n + (int64_t)kB * g.ldb] : g.B[kB + (int64_t)n * g.ldb];
-            Bs[kq][nn] = bv;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
         }
+        if (more) sstore(buf ^ 1);
         __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-            double a[4], b[4];
-#pragma unroll
-            for (int p = 0; p < 4; ++p) a[p] = As[kk][tx + 16 * p];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) b[q] = Bs[kk][ty + 16 * q];
-#pragma unroll
-            for (int p = 0; p < 4; ++p)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) acc[p][q] = fma(a[p], b[q], acc[p][q]);
-        }
-        __syncthreads();
+        buf ^= 1;
     }
 #pragma unroll
-    for (int p = 0; p < 4; ++p)
+    for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int m = m0 + tx + 16 * p, n = n0 + ty + 16 * q;
+        for (int j = 0; j < 8; ++j) {
+            const int m = m0 + tr * 8 + i, n = n0 + tc * 8 + j;
             if (m >= g.M || n >= g.N) continue;
             if (ws) {
-                ws[((int64_t)blockIdx.z * g.N + n) * g.M + m] = acc[p][q];
+                ws[((int64_t)blockIdx.z * g.N + n) * g.M + m] = acc[i][j];
                 continue;
             }
             const int64_t o = m + (int64_t)n * g.ldo;
-            double v = g.alpha * acc[p][q];
+            double v = g.alpha * acc[i][j];
             if (g.X) v += g.beta * g.X[o];
             if (g.Y) v += g.gamma * g.Y[o];
             g.O[o] = v;
@@ -170,74 +225,23 @@ struct GemmWs {
     DevBuf ws;
 };
 
-// O = beta X + gamma Y (either may be NULL), element-wise over M x N.
-__global__ void k_axpby(Gemm g) {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (int64_t)g.M * g.N) return;
-    const int m = (int)(idx % g.M), n = (int)(idx / g.M);
-    const int64_t o = m + (int64_t)n * g.ldo;
-    double v = 0.0;
-    if (g.X) v += g.beta * g.X[o];
-    if (g.Y) v += g.gamma * g.Y[o];
-    g.O[o] = v;
-}
-
-// cuBLAS handle of the current device (created on first use).
-int blas_handle(cublasHandle_t *out) {
-    static std::mutex mu;
-    static cublasHandle_t h[64] = {};
-    int dev = 0;
-    CREST_CUDA_TRY(cudaGetDevice(&dev));
-    CREST_REQUIRE(dev >= 0 && dev < 64, CREST_ERUNTIME, "device index %d out of range", dev);
-    std::lock_guard<std::mutex> lock(mu);
-    if (!h[dev]) {
-        const cublasStatus_t r = cublasCreate(&h[dev]);
-        CREST_REQUIRE(r == CUBLAS_STATUS_SUCCESS, CREST_ECUDA, "cublasCreate failed (%d)", (int)r);
-    }
-    *out = h[dev];
-    return CREST_OK;
-}
-
-// Products with a long inner dimension (K >= 512: the filter's C times a
-// d x q block, and the q x q Gram matrices of a d x q block) go to cuBLAS
-// DGEMM; the epilogue's extra terms are formed first in O.
-int gemm_blas(const Gemm &g, cudaStream_t st) {
-    cublasHandle_t h;
-    CREST_TRY(blas_handle(&h));
-    CREST_REQUIRE(cublasSetStream(h, st) == CUBLAS_STATUS_SUCCESS, CREST_ECUDA, "cublasSetStream failed");
-    double beta = 0.0;
-    if (g.Y || (g.X && g.X != g.O)) {
-        k_axpby<<<(unsigned)ceil_div((int64_t)g.M * g.N, 256), 256, 0, st>>>(g);
-        CREST_CUDA_TRY(cudaGetLastError());
-        beta = 1.0;
-    } else if (g.X == g.O && g.X) {
-        beta = g.beta;
-    }
-    const cublasStatus_t r =
-        cublasDgemm(h, g.tA ? CUBLAS_OP_T : CUBLAS_OP_N, g.tB ? CUBLAS_OP_T : CUBLAS_OP_N, g.M, g.N, g.K, &g.alpha,
-                    g.A, g.lda, g.B, g.ldb, &beta, g.O, g.ldo);
-    CREST_REQUIRE(r == CUBLAS_STATUS_SUCCESS, CREST_ECUDA, "cublasDgemm failed (%d)", (int)r);
-    return CREST_OK;
-}
-
 int gemm(const Gemm &g, GemmWs &w, cudaStream_t st) {
     prof::Scope ps("eig_gemm_fp64", st);
-    if (g.K >= 512) return gemm_blas(g, st);
-    const int mt = (int)ceil_div(g.M, 64), nt = (int)ceil_div(g.N, 64);
+    const int mt = (int)ceil_div(g.M, kGM), nt = (int)ceil_div(g.N, kGN);
     int ksplit = 1;
-    if (g.K > 0) {
-        const int want = (int)ceil_div(2 * device_sms(), mt * nt);
+    if (g.K > 0) {  // about one CTA per SM, slices of at least 64
+        const int want = (int)ceil_div(device_sms(), mt * nt);
         ksplit = std::max(1, std::min(want, (int)ceil_div(g.K, 64)));
     }
     if (ksplit == 1) {
-        k_gemm<<<dim3(mt, nt, 1), 256, 0, st>>>(g, std::max(g.K, 1), nullptr);
+        k_gemm<<<dim3(mt, nt, 1), 128, 0, st>>>(g, std::max(g.K, 1), nullptr);
         CREST_CUDA_TRY(cudaGetLastError());
         return CREST_OK;
     }
-    const int kchunk = (int)round_up(ceil_div(g.K, ksplit), 16);
+    const int kchunk = (int)round_up(ceil_div(g.K, ksplit), kGK);
     ksplit = (int)ceil_div(g.K, kchunk);
     CREST_TRY(w.ws.ensure(sizeof(double) * (size_t)ksplit * g.M * g.N));
-    k_gemm<<<dim3(mt, nt, ksplit), 256, 0, st>>>(g, kchunk, w.ws.as<double>());
+    k_gemm<<<dim3(mt, nt, ksplit), 128, 0, st>>>(g, kchunk, w.ws.as<double>());
     CREST_CUDA_TRY(cudaGetLastError());
     k_gemm_reduce<<<(unsigned)ceil_div((int64_t)g.M * g.N, 256), 256, 0, st>>>(g, ksplit, w.ws.as<double>());
     CREST_CUDA_TRY(cudaGetLastError());

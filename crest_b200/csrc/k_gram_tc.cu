@@ -376,6 +376,311 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_bf16x3(const __grid_consta
     }
 }
 
+// ------------------------------------------------------ CTA-pair form
+// The same contraction on pairs of SMs (tcgen05 cta_group::2): a cluster of
+// two CTAs owns a 256 x 256 block (bi, bj) of G, M = 256 rows split 128 per
+// CTA, N = 256 columns whose B operand is split 128 per CTA, so every CTA
+// stages 128 a-genes and 128 b-genes per stage -- the operand bytes per
+// output halve against one CTA per 128 x 128 block, which is what bounded
+// that form (L2 -> shared memory).  Each CTA's TMEM holds its 128 rows x 256
+// columns of the FP32 accumulator, two of them (all 512 columns).  The
+// cells of a launch are split in two halves (pairs 2t and 2t + 1 of tile t)
+// so the 36 blocks of d = 2048 keep 144 SMs busy; half 1 adds into a second
+// FP64 Gram (gram_aux), folded into G once per pass.
+//
+// Roles: warp 0 of each CTA loads its own operand halves (TMA, cta_group::2
+// form, completing on the leader CTA's full barrier, which the leader's
+// producer arms with both CTAs' bytes); warp 1 of the leader issues the
+// MMAs and the commits, multicast to both CTAs' barriers; warps 2-9 of both
+// CTAs read their TMEM rows every period (fold stages of 64 cells) and add
+// them into FP32 register sums (one row, 128 columns per thread), and
+// release the accumulator on the leader's barrier (local and remote
+// arrivals).  FP32 register sums over a launch's periods are correctly
+// rounded adds of at most 32 period results; the FP64 update of G at the
+// end applies the shift correction once (in half 0).
+namespace pair {
+
+constexpr int kN = 256;                       // block edge (M = N)
+constexpr int kHalfRows = 128;                // rows (and B columns) per CTA
+constexpr int kStageBytes = 4 * kOperandBytes;  // A_hi, A_lo, B_hi, B_lo of this CTA: 64 KB
+constexpr int kAccCols = 256;
+constexpr int kAccBufs = 2;
+
+__device__ __forceinline__ uint32_t cta_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// shared::cluster address of the same shared-memory location in CTA `rank`
+__device__ __forceinline__ uint32_t mapa(uint32_t addr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(addr), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void arrive_cluster(uint32_t cluster_addr) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_addr) : "memory");
+}
+
+__device__ __forceinline__ bool try_cluster(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(20000u)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait (as mbar_wait) with cluster-scope acquire.
+__device__ __forceinline__ bool wait(uint64_t *bar, uint32_t parity, int *err, int code) {
+    if (try_cluster(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer();
+    for (uint32_t n = 1;; ++n) {
+        if (try_cluster(bar, parity)) return true;
+        if ((n & 63u) == 0) {
+            if (globaltimer() - t0 > kWaitNs) {
+                atomicCAS(err, 0, code);
+                return false;
+            }
+            if (*(volatile int *)err) return false;
+        }
+    }
+}
+
+__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
+    int got = 0;
+    if ((threadIdx.x & 31) == 0) got = wait(bar, parity, err, code) ? 1 : 0;
+    return __shfl_sync(0xffffffffu, got, 0) != 0;
+}
+
+// TMA load into this CTA's shared memory, completing on the barrier at the
+// shared::cluster address bar (the leader's).
+__device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, uint32_t bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], "
+        "[%2];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y)
+        : "memory");
+}
+
+// instruction descriptor: as kIdesc with M = 256 (the pair), N = 256
+constexpr uint32_t kIdesc2 = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                             ((uint32_t)(kN >> 3) << 17) | ((uint32_t)(kN >> 4) << 24);
+
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5, %5, %5, %5, %5}, p;\n\t}" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(kIdesc2), "r"(accumulate), "r"(0u));
+}
+
+// arrive on barrier `bar` (same offset) in both CTAs once this thread's MMAs complete
+__device__ __forceinline__ void commit_both(uint64_t *bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"((uint16_t)3)
+        : "memory");
+}
+
+struct Args {
+    int64_t d, d_pad;
+    int n_stages;          // 64-cell stages of the launch
+    int m_pad;             // cells in the tile (row offset of the lo plane)
+    int fold;              // stages per FP32 TMEM period
+    int nb;                // 256-blocks along d_pad
+    const double *bias;    // [d] or nullptr
+    const double *colsum;  // [d]
+    const int64_t *n_kept;
+    double *G, *G_aux;     // [d x d]: cell halves 0 and 1
+    int *err;
+};
+
+__global__ void __launch_bounds__(kThreads, 1) k_syrk_pair(const __grid_constant__ CUtensorMap tmap, Args a) {
+    extern __shared__ uint8_t smem_dyn[];
+    __shared__ __align__(8) uint64_t full_bar[kStages], empty_bar[kStages], acc_full[kAccBufs], acc_empty[kAccBufs];
+    __shared__ uint32_t tmem_base_sh;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cta_rank();
+    const bool leader = rank == 0;
+    const int pair_id = blockIdx.x >> 1;
+    const int t = pair_id >> 1, half = pair_id & 1;
+    int bi, bj;
+    tri_decode(t, a.nb, bi, bj);
+    const bool diag = bi == bj;
+    const int s_lo = half == 0 ? 0 : a.n_stages / 2, s_hi = half == 0 ? a.n_stages / 2 : a.n_stages;
+    const int n_my = s_hi - s_lo;
+    const int n_periods = (n_my + a.fold - 1) / a.fold;
+    const uint32_t raw = smem_u32(smem_dyn);
+    uint8_t *ring = smem_dyn + (((raw + 1023u) & ~1023u) - raw);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        for (int b = 0; b < kAccBufs; ++b) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 2 * kEpiWarps);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    }
+    tc_fence_before();
+    cluster_sync();  // barriers initialised and TMEM allocated in both CTAs
+    tc_fence_after();
+    const uint32_t tmem = tmem_base_sh;
+
+    if (warp == 0) {
+        // ------------------------------------------------------ producer
+        const uint32_t bytes_cta = diag ? 2 * kOperandBytes : 4 * kOperandBytes;
+        const int xa = bi * kN + (int)rank * kHalfRows, xb = bj * kN + (int)rank * kHalfRows, lo_off = a.m_pad;
+        int issued = 0;
+        for (int i = 0; i < n_my; ++i) {
+            const int s = i % kStages;
+            if (i >= kStages && !warp_wait(&empty_bar[s], ((i / kStages) - 1) & 1, a.err, 11)) break;
+            if (lane == 0) {
+                uint8_t *st = ring + (size_t)s * kStageBytes;
+                const uint32_t fb = mapa(smem_u32(&full_bar[s]), 0);
+                if (leader) mbar_expect_tx(&full_bar[s], 2 * bytes_cta);
+                const int y = (s_lo + i) * kStageCells;
+                tma_load(st, &tmap, fb, xa, y);
+                tma_load(st + kBoxBytes, &tmap, fb, xa + kHalf, y);
+                tma_load(st + kOperandBytes, &tmap, fb, xa, lo_off + y);
+                tma_load(st + kOperandBytes + kBoxBytes, &tmap, fb, xa + kHalf, lo_off + y);
+                if (!diag) {
+                    tma_load(st + 2 * kOperandBytes, &tmap, fb, xb, y);
+                    tma_load(st + 2 * kOperandBytes + kBoxBytes, &tmap, fb, xb + kHalf, y);
+                    tma_load(st + 3 * kOperandBytes, &tmap, fb, xb, lo_off + y);
+                    tma_load(st + 3 * kOperandBytes + kBoxBytes, &tmap, fb, xb + kHalf, lo_off + y);
+                }
+            }
+            __syncwarp();
+            issued = i + 1;
+        }
+        // drain: the last stages' releases (MMA commits) land before exit
+        for (int i = max(0, issued - kStages); i < issued; ++i)
+            if (!warp_wait(&empty_bar[i % kStages], (i / kStages) & 1, a.err, 15)) break;
+    } else if (warp == 1) {
+        // --------------------------------------------- MMA issuer (leader)
+        if (leader) {
+            bool ok = true;
+            for (int p = 0; p < n_periods && ok; ++p) {
+                const int buf = p % kAccBufs;
+                if (p >= kAccBufs && !warp_wait(&acc_empty[buf], ((p / kAccBufs) - 1) & 1, a.err, 12)) break;
+                const uint32_t d_tmem = tmem + (uint32_t)(buf * kAccCols);
+                const int i0 = p * a.fold, i1 = min(n_my, i0 + a.fold);
+                for (int i = i0; i < i1; ++i) {
+                    const int s = i % kStages;
+                    if (!warp_wait(&full_bar[s], (i / kStages) & 1, a.err, 13)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    if (lane == 0) {
+                        const uint32_t st = smem_u32(ring + (size_t)s * kStageBytes);
+                        const uint32_t a_hi = st, a_lo = st + kOperandBytes;
+                        const uint32_t b_hi = diag ? a_hi : st + 2 * kOperandBytes;
+                        const uint32_t b_lo = diag ? a_lo : st + 3 * kOperandBytes;
+#pragma unroll
+                        for (int kk = 0; kk < kStageCells / 16; ++kk) {
+                            const uint32_t off = kk * 16 * 128;
+                            const uint32_t first = (i == i0 && kk == 0) ? 0u : 1u;
+                            mma(d_tmem, umma_desc(a_hi + off), umma_desc(b_hi + off), first);
+                            mma(d_tmem, umma_desc(a_hi + off), umma_desc(b_lo + off), 1u);
+                            mma(d_tmem, umma_desc(a_lo + off), umma_desc(b_hi + off), 1u);
+                        }
+                        commit_both(&empty_bar[s]);
+                    }
+                    __syncwarp();
+                }
+                if (ok && lane == 0) commit_both(&acc_full[buf]);
+                __syncwarp();
+            }
+        }
+    } else {
+        // ------------------------------------------------------ epilogue
+        const int q = warp & 3;         // TMEM lane quadrant of this warp
+        const int h = (warp - 2) >> 2;  // columns 128 h .. 128 h + 127
+        const int row = q * 32 + lane;
+        float acc[128];
+#pragma unroll
+        for (int j = 0; j < 128; ++j) acc[j] = 0.0f;
+        bool ok = true;
+        const uint32_t empty_leader[2] = {mapa(smem_u32(&acc_empty[0]), 0), mapa(smem_u32(&acc_empty[1]), 0)};
+        for (int p = 0; p < n_periods; ++p) {
+            const int buf = p % kAccBufs;
+            if (!warp_wait(&acc_full[buf], (p / kAccBufs) & 1, a.err, 14)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * kAccCols + h * 128);
+#pragma unroll
+            for (int g = 0; g < 8; ++g) {
+                float v[16];
+                tmem_ld16(taddr + 16 * g, v);
+                tmem_wait_ld();
+#pragma unroll
+                for (int j = 0; j < 16; ++j) acc[16 * g + j] += v[j];
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) arrive_cluster(empty_leader[buf]);
+        }
+        // the ring is idle: every MMA (which reads both CTAs' stages) has
+        // completed before the last accumulator was committed
+        float *stage = reinterpret_cast<float *>(ring);
+        constexpr int kPitch = kN + 1;
+        if (ok) {
+#pragma unroll
+            for (int j = 0; j < 128; ++j) stage[row * kPitch + h * 128 + j] = acc[j];
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(kEpiWarps * 32) : "memory");
+        if (ok && !*(volatile int *)a.err) {
+            const int e = warp - 2;
+            const bool corr = half == 0 && a.bias;
+            double *G = half == 0 ? a.G : a.G_aux;
+            const double nk = (double)*a.n_kept;
+            for (int r = e; r < kHalfRows; r += kEpiWarps) {
+                const int64_t ga = (int64_t)bi * kN + (int64_t)rank * kHalfRows + r;
+                if (ga >= a.d) break;
+                const double ba = corr ? a.bias[ga] : 0.0, ca = corr ? a.colsum[ga] : 0.0;
+                double *grow = G + ga * a.d;
+                for (int cc = lane; cc < kN; cc += 32) {
+                    const int64_t gb = (int64_t)bj * kN + cc;
+                    if (gb >= a.d || gb < ga) continue;
+                    double v = (double)stage[r * kPitch + cc];
+                    if (corr) v = v - ba * a.colsum[gb] - ca * a.bias[gb] - nk * ba * a.bias[gb];
+                    grow[gb] += v;
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    cluster_sync();  // both CTAs done with TMEM, barriers and shared memory
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+    }
+}
+
+}  // namespace pair
+
 // --------------------------------------------------------------- host side
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -401,6 +706,12 @@ static ErrFlag g_tc_err[64];
 // default 128 cells; at 1M cells periods of 64, 128 and 256 cells all keep
 // the top-50 subspace within 0.007 degree of the FP64 Gram, 512 cells drift
 // past 0.01 degree).
+// CTA-pair SYRK (default) or one CTA per 128 x 128 block (CREST_TC_PAIR=0).
+bool tc_pair_enabled() {
+    const char *e = getenv("CREST_TC_PAIR");
+    return !(e && e[0] == '0');
+}
+
 int tc_fold_stages() {
     const char *e = getenv("CREST_TC_FOLD");
     int v = e ? atoi(e) : 128 / kStageCells;
@@ -460,11 +771,63 @@ int syrk_bf16x3_fold(const GramWork &w, int64_t m_pad, const DevScale &t, double
     a.n_kept = w.n_kept;
     a.G = gram;
     a.err = err;
+    if (tc_pair_enabled() && w.gram_aux && w.d_pad % pair::kN == 0) {
+        pair::Args b;
+        b.d = w.d;
+        b.d_pad = w.d_pad;
+        b.n_stages = a.n_stages;
+        b.m_pad = a.m_pad;
+        b.fold = a.fold;
+        b.nb = (int)(w.d_pad / pair::kN);
+        b.bias = a.bias;
+        b.colsum = a.colsum;
+        b.n_kept = a.n_kept;
+        b.G = gram;
+        b.G_aux = w.gram_aux;
+        b.err = err;
+        const size_t smem = 1024 + (size_t)kStages * pair::kStageBytes;
+        prof::Scope ps("syrk_bf16x3_tcgen05_pair", st);
+        CREST_TRY(ensure_smem_attr((const void *)pair::k_syrk_pair, smem));
+        const int tiles = b.nb * (b.nb + 1) / 2;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(tiles * 4), 1, 1);  // two cell halves x two CTAs per tile
+        cfg.blockDim = dim3(kThreads, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CREST_CUDA_TRY(cudaLaunchKernelEx(&cfg, pair::k_syrk_pair, map, b));
+        return CREST_OK;
+    }
     const size_t smem = 1024 + (size_t)kStages * kStageBytes;
     prof::Scope ps("syrk_bf16x3_tcgen05", st);
     CREST_TRY(ensure_smem_attr((const void *)k_syrk_bf16x3, (size_t)smem));
     const int tiles = a.nb * (a.nb + 1) / 2;
     k_syrk_bf16x3<<<tiles, kThreads, smem, st>>>(map, a);
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
+}
+
+// gram += aux; aux = 0 (the second cell half of the CTA-pair SYRK).
+__global__ void k_gram_fold(double *__restrict__ gram, double *__restrict__ aux, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = aux[i];
+    if (v != 0.0) {
+        gram[i] += v;
+        aux[i] = 0.0;
+    }
+}
+
+int gram_aux_fold(const GramWork &w, double *gram, cudaStream_t st) {
+    if (!w.gram_aux || w.d == 0) return CREST_OK;
+    const int64_t n = w.d * w.d;
+    k_gram_fold<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(gram, w.gram_aux, n);
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
 }

@@ -99,6 +99,8 @@ struct GramWork {
                             // precision, so the (repeated) zeros are stored exactly
     int *status;            // [1] bit 1: a cell holds one column twice; bit 2: a cell could not
                             // be checked (unsorted, more HVG entries than the densify queue)
+    double *gram_aux;       // [d x d] BF16X3: Gram of the second cell half of each tile (CTA-pair
+                            // SYRK), zero between passes; folded by gram_aux_fold
 };
 
 size_t gram_tile_bytes(int precision, int64_t d_pad, int64_t m_cap);
@@ -112,6 +114,8 @@ int launch_syrk_fold(const GramWork &w, int64_t m, const DevScale &t, double *gr
                      cudaStream_t st);
 // Non-zero error word of the tensor-core Gram pipeline -> CREST_ETIMEOUT (and cleared).
 int tc_check_error();
+// gram += gram_aux, gram_aux = 0: once at the end of every Gram pass.
+int gram_aux_fold(const GramWork &w, double *gram, cudaStream_t st);
 // shift[j] = bias[j] rounded to the tile precision (the stored value of zeros).
 int launch_tile_shift(const GramWork &w, const DevScale &t, cudaStream_t st);
 

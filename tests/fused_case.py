@@ -8,8 +8,8 @@ import torch
 from crest_b200 import synth
 
 
-def make_case(n=3000, d=400, k=24, max_value=10.0, seed=0):
-    p = synth.make_params(n, d, 5, 0.5, 60.0, seed=seed)
+def make_case(n=3000, d=400, k=24, max_value=10.0, seed=0, nnz_per_cell=60.0, clusters=5, dispersion=0.5):
+    p = synth.make_params(n, d, clusters, dispersion, nnz_per_cell, seed=seed)
     from oracle import synth as osynth
     indptr, indices, data = osynth.generate(p)
     rng = np.random.default_rng(seed + 1)
@@ -28,12 +28,14 @@ def make_case(n=3000, d=400, k=24, max_value=10.0, seed=0):
 
 
 def reference(c, values, sf, W):
-    """FP64 torch restatement of the map (float64 tensors, autograd-able)."""
+    """FP64 torch restatement of the map (float64 tensors, autograd-able), on
+    the device of `values`."""
     n = c["n"]
-    cell = torch.as_tensor(np.repeat(np.arange(n), np.diff(c["indptr"])))
-    g = torch.as_tensor(c["indices"].astype(np.int64))
-    mean = torch.as_tensor(c["mean"])
-    std = torch.as_tensor(c["std"])
+    dev = values.device
+    cell = torch.as_tensor(np.repeat(np.arange(n), np.diff(c["indptr"])), device=dev)
+    g = torch.as_tensor(c["indices"].astype(np.int64), device=dev)
+    mean = torch.as_tensor(c["mean"], device=dev)
+    std = torch.as_tensor(c["std"], device=dev)
     mv = c["max_value"]
     y = values / sf[cell]
     z = (torch.log1p(y) - mean[g]) / std[g]
@@ -42,7 +44,7 @@ def reference(c, values, sf, W):
         z = torch.clamp(z, -mv, mv)
         b = torch.clamp(b, -mv, mv)
     s = z - b
-    scores = torch.zeros((n, W.shape[1]), dtype=torch.float64)
+    scores = torch.zeros((n, W.shape[1]), dtype=torch.float64, device=dev)
     scores.index_add_(0, cell, s[:, None] * W[g])
     return scores
 
@@ -51,13 +53,13 @@ def loss_of(scores, wts):
     return (wts * scores * scores).sum()
 
 
-def ref_run(c):
-    values = torch.tensor(c["values"].astype(np.float64), requires_grad=True)
-    sf = torch.tensor(c["sf"].astype(np.float64), requires_grad=True)
-    W = torch.tensor(c["W"].astype(np.float64), requires_grad=True)
+def ref_run(c, device="cpu"):
+    values = torch.tensor(c["values"].astype(np.float64), requires_grad=True, device=device)
+    sf = torch.tensor(c["sf"].astype(np.float64), requires_grad=True, device=device)
+    W = torch.tensor(c["W"].astype(np.float64), requires_grad=True, device=device)
     scores = reference(c, values, sf, W)
-    loss_of(scores, torch.tensor(c["wts"])).backward()
-    return scores.detach(), values.grad, sf.grad, W.grad
+    loss_of(scores, torch.tensor(c["wts"], device=device)).backward()
+    return scores.detach().cpu(), values.grad.cpu(), sf.grad.cpu(), W.grad.cpu()
 
 
 def rel(a, b):

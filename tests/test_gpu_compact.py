@@ -148,3 +148,35 @@ def test_duplicate_entries_rejected_per_chunk(small_counts):
                                 s["mean"], s["std"], 10.0, precision="fp32")
     # the caller's accumulators are left as they were
     assert np.all(G == 0.5) and np.all(cs == 0.5)
+
+
+@pytest.mark.parametrize("pair", ["1", "0"])
+def test_bf16x3_gram_both_syrk_forms(pbmc_counts, monkeypatch, pair):
+    """The CTA-pair tensor-core SYRK (256 x 256 blocks, two cell halves) and the
+    one-CTA form (128 x 128 blocks) against the FP64 Gram of the same plan API,
+    d = 2000 HVG columns (36 pair blocks): centred covariances within 5e-6."""
+    monkeypatch.setenv("CREST_TC_PAIR", pair)
+    indptr, indices, data, n_genes = pbmc_counts[:4]
+    s = setup((indptr, indices, data, n_genes), 9, d_frac=0.0)
+    rng = np.random.default_rng(9)
+    mask = np.zeros(s["nv"], bool)
+    mask[rng.choice(s["nv"], 2000, replace=False)] = True
+    sub = np.full(s["nv"], -1, np.int32)
+    sub[mask] = np.arange(2000, dtype=np.int32)
+    st = np.zeros((s["nv"], 5))
+    oracle.gene_stats(indices, data, s["cm"], s["gm"], 1e4, True, None, indptr, 0, st)
+    nk = s["nr"]
+    mean = st[:, 0] / nk
+    std = np.sqrt(np.maximum((st[:, 1] - nk * mean * mean) / (nk - 1), 0))
+    std[std == 0] = 1
+    s.update(d=2000, sub=sub, mean=np.ascontiguousarray(mean[mask]), std=np.ascontiguousarray(std[mask]))
+    cov = []
+    for prec in ("fp64", "bf16x3"):
+        p, dm, _ = plan_gram(s, "device", prec)
+        G, c = p.gram(), p.results()[3]
+        S = np.triu(G) + np.triu(G, 1).T
+        cov.append((S - np.outer(c, c) / nk) / (nk - 1))
+        p.close()
+        dm.close()
+    err = np.linalg.norm(cov[1] - cov[0]) / np.linalg.norm(cov[0])
+    assert err < 5e-6, err

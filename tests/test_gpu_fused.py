@@ -44,6 +44,20 @@ def test_forward_and_gradients_match_fp64_reference(k, max_value):
     assert rel(gW, rW) <= 1e-4
 
 
+def test_differentiation_workload_shape():
+    """The differentiation workload at its own shape: 50,000 cells x 2,000 HVG
+    genes (~200 stored entries per cell), k = 50, scale max 10; the FP64
+    reference runs with float64 PyTorch ops on the GPU."""
+    c = make_case(n=50_000, d=2_000, k=50, max_value=10.0, seed=4, nnz_per_cell=200.0, clusters=20,
+                  dispersion=0.2)
+    s_gpu, gx, gsf, gW = gpu_run(c)
+    s_ref, rx, rsf, rW = ref_run(c, device="cuda")
+    assert rel(s_gpu, s_ref) <= 1e-5
+    assert rel(gx, rx) <= 1e-4
+    assert rel(gsf, rsf) <= 1e-4
+    assert rel(gW, rW) <= 1e-4
+
+
 def test_out_of_range_gene_id_is_rejected():
     c = make_case(n=50, d=40, k=8)
     c["indices"][3] = c["d"] + 5
