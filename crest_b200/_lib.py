@@ -61,6 +61,8 @@ _SIGS = {
     "crest_qc": [P, P, I64, P, P, P, I64, P, P],
     "crest_qc_static": [P, P, I64, P, P, P, I64, P, P],
     "crest_gene_stats": [P, I64, P],
+    "crest_group_gene_sums": [P, P, I64, I64, I64, P, P, P, P],
+    "crest_group_gene_totals": [P, P, I64, I64, I64, P],
     "crest_gram_accumulate": [P, P, I64, P, I64, P, P, I32],
     "crest_pca_from_gram": [P, P, I64, I64, I64, P, P, P, P],
     "crest_project": [P, P, I64, P, I64, I64, P, P, I64],
@@ -69,6 +71,7 @@ _SIGS = {
     "crest_matrix_info": [P, P, P, P],
     "crest_matrix_qc": [P, P, P, P, I64, I64, P, P, P, P, P],
     "crest_matrix_gene_stats": [P, P, P, D, I32, I64, P],
+    "crest_matrix_group_gene_sums": [P, P, P, D, I32, P, I64, I64, I64, P, P, P, P],
     "crest_pca_create": [P, I64, I32],
     "crest_pca_free": [P],
     "crest_pca_accumulate": [P, P, P, P, D, I32, P, I64, P],

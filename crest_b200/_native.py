@@ -19,7 +19,8 @@ import numpy as np
 from . import _lib
 from ._lib import carray, ptr
 
-__all__ = ["qc", "gene_stats", "gram_accumulate", "pca_from_gram", "project"]
+__all__ = ["qc", "gene_stats", "gram_accumulate", "pca_from_gram", "project", "group_gene_sums",
+           "group_gene_totals", "t_pvalues"]
 
 
 def _chunk(genes, values, cell_map, gene_map, target_sum, log1p, cells, indptr, first_cell):
@@ -158,3 +159,51 @@ def pca_from_gram(gram, colsum, n, k):
         raise RuntimeError(_lib.load().crest_last_error().decode(errors="replace"))
     _lib.check(rc)
     return vals, vecs, float(total[0])
+
+
+def group_gene_sums(genes, values, cell_map, gene_map, target_sum, log1p, cells, indptr, first_cell,
+                    group_of_row, sum, sumsq, nnz, clip=None):
+    """Accumulate per (group, var) sums, sums of squares and nnz (each (n_groups, n_vars)) of the
+    transformed values; ``clip`` (n_groups, n_vars) caps each value first (src/py.rs:311-338)."""
+    ch, keep, nr, nv = _chunk(genes, values, cell_map, gene_map, target_sum, log1p, cells, indptr, first_cell)
+    gr = carray(group_of_row, np.uint32, "group_of_row")
+    s, q, z = _mut(sum, np.float64, "sum"), _mut(sumsq, np.float64, "sumsq"), _mut(nnz, np.float64, "nnz")
+    if s.ndim != 2 or s.shape[1] != nv or q.shape != s.shape or z.shape != s.shape or len(gr) < nr:
+        raise ValueError("sum, sumsq, nnz must be (n_groups, n_vars); group_of_row (n_rows,)")
+    if bool(np.any((gr != np.iinfo(np.uint32).max) & (gr >= s.shape[0]))):
+        raise ValueError("group id out of range")
+    c = None
+    if clip is not None:
+        c = carray(clip, np.float64, "clip")
+        if c.size != s.size:
+            raise ValueError("clip must be (n_groups, n_vars)")
+    _lib.call("crest_group_gene_sums", C.byref(ch), ptr(gr), len(gr), s.shape[0], nv, ptr(c), ptr(s), ptr(q),
+              ptr(z))
+
+
+def group_gene_totals(genes, values, cell_map, gene_map, target_sum, log1p, cells, indptr, first_cell,
+                      group_of_row, sum):
+    """Accumulate per (group, var) sums only, (n_groups, n_vars): pseudobulk aggregation (src/py.rs:340-357)."""
+    ch, keep, nr, nv = _chunk(genes, values, cell_map, gene_map, target_sum, log1p, cells, indptr, first_cell)
+    gr = carray(group_of_row, np.uint32, "group_of_row")
+    s = _mut(sum, np.float64, "sum")
+    if s.ndim != 2 or s.shape[1] != nv or len(gr) < nr:
+        raise ValueError("sum must be (n_groups, n_vars); group_of_row (n_rows,)")
+    if bool(np.any((gr != np.iinfo(np.uint32).max) & (gr >= s.shape[0]))):
+        raise ValueError("group id out of range")
+    _lib.call("crest_group_gene_totals", C.byref(ch), ptr(gr), len(gr), s.shape[0], nv, ptr(s))
+
+
+def t_pvalues(t, df):
+    """Two-sided p-values of Student's t, 2 * sf(|t|, df) capped at 1; NaN for a
+    non-finite t or df <= 0 (src/py.rs:413-427).  Host arithmetic over one value per
+    gene (scipy's Student t distribution function)."""
+    from scipy.special import stdtr
+    t = np.asarray(t, np.float64)
+    df = np.asarray(df, np.float64)
+    if t.shape != df.shape:
+        raise ValueError("t, df must have equal length")
+    ok = np.isfinite(t) & (df > 0)
+    p = np.full(t.shape, np.nan)
+    p[ok] = np.minimum(2.0 * stdtr(df[ok], -np.abs(t[ok])), 1.0)
+    return p

@@ -208,11 +208,14 @@ class BioFrame:
         return [str(x) for x in self.var["gene_id"].tolist()]
 
     def __repr__(self) -> str:
-        kind = type(self.store).__name__
-        ops = ", ".join(o[0] for o in self.ops) or "raw counts"
-        return (f"BioFrame {self.n_obs} cells x {self.n_vars} genes ({kind}; {ops})\n"
-                f"    obs: {list(self.obs.columns)}\n    var: {list(self.var.columns)}\n"
-                f"    obsm: {list(self.obsm)}  uns: {list(self.uns)}")
+        pending = [o[0] for o in self.ops]
+        lines = [f"<BioFrame: {self.n_obs:,} cells, {self.n_vars:,} genes, store={type(self.store).__name__}, "
+                 f"lazy ops={pending if pending else 'none'}>"]
+        for label, keys in (("obs", self.obs.columns), ("var", self.var.columns), ("obsm", self.obsm),
+                            ("varm", self.varm), ("uns", self.uns)):
+            if len(keys):
+                lines.append(f"  {label}: " + ", ".join(map(str, keys)))
+        return "\n".join(lines)
 
     # ---- maps from store ids to current rows (crest/core.py:244-263)
     def _cell_map(self) -> np.ndarray:
@@ -252,15 +255,20 @@ class BioFrame:
         return self.store.device_matrix() if isinstance(self.store, CSRStore) else None
 
     # ---- subsetting
+    # uns entries whose contents are indexed by cells: stale once cells are dropped
+    _PER_CELL_UNS = ("neighbors",)
+
     def _subset(self, obs_mask=None, var_mask=None) -> "BioFrame":
-        obs = self.obs if obs_mask is None else self.obs[np.asarray(obs_mask, bool)].reset_index(drop=True)
-        var = self.var if var_mask is None else self.var[np.asarray(var_mask, bool)].reset_index(drop=True)
-        obsm = {k: v[obs_mask] for k, v in self.obsm.items()} if obs_mask is not None else dict(self.obsm)
-        varm = {k: v[var_mask] for k, v in self.varm.items()} if var_mask is not None else dict(self.varm)
-        uns = dict(self.uns)
-        if obs_mask is not None:
-            uns.pop("neighbors", None)
-        return BioFrame(self.store, obs, var, obsm, varm, uns, list(self.ops), self.chunk_nnz)
+        """A view keeping the masked cells / genes; the store is shared, no counts are copied."""
+        def pick(frame, mask):
+            return frame if mask is None else frame.loc[np.asarray(mask, bool)].reset_index(drop=True)
+
+        def pick_rows(arrays, mask):
+            return dict(arrays) if mask is None else {key: a[np.asarray(mask, bool)] for key, a in arrays.items()}
+
+        uns = {key: v for key, v in self.uns.items() if obs_mask is None or key not in self._PER_CELL_UNS}
+        return BioFrame(self.store, pick(self.obs, obs_mask), pick(self.var, var_mask), pick_rows(self.obsm, obs_mask),
+                        pick_rows(self.varm, var_mask), uns, list(self.ops), self.chunk_nnz)
 
     def filter_cells(self, mask) -> "BioFrame":
         """Keep cells where the boolean mask holds."""

@@ -24,10 +24,32 @@ void set_error(const char *fmt, ...) {
 }
 const char *last_error() { return g_err.c_str(); }
 
+// Failure-injection hook for tests (host side): CREST_INJECT_ALLOC_FAIL=N
+// makes the N-th device allocation from now on fail as if the device were
+// out of memory (read on every allocation; off by default).
+static bool injected_alloc_failure() {
+    static std::mutex mu;
+    static long countdown = 0;
+    static std::string seen;
+    std::lock_guard<std::mutex> lock(mu);
+    const char *e = getenv("CREST_INJECT_ALLOC_FAIL");
+    const std::string v = e ? e : "";
+    if (v != seen) {  // a new setting re-arms the countdown
+        seen = v;
+        countdown = v.empty() ? 0 : atol(v.c_str());
+    }
+    if (countdown <= 0) return false;
+    return --countdown == 0;
+}
+
 int DevBuf::ensure(size_t bytes) {
     if (bytes <= cap && ptr) return CREST_OK;
     release();
     size_t want = bytes < 256 ? 256 : bytes;
+    if (injected_alloc_failure()) {
+        set_error("device allocation of %zu bytes failed: out of memory (injected)", want);
+        return CREST_ENOMEM;
+    }
     cudaError_t e = cudaMalloc(&ptr, want);
     if (e != cudaSuccess) {
         ptr = nullptr;
@@ -466,6 +488,60 @@ int crest_pca_from_gram(const double *gram, const double *colsum, int64_t d, int
     CREST_REQUIRE(es.converged, CREST_ERUNTIME, "eigensolver did not converge (residual %.3g after %d iterations)",
                   es.residual, es.iters);
     return CREST_OK;
+}
+
+int crest_group_gene_sums(const crest_chunk *chunk, const uint32_t *group_of_row, int64_t n_group_rows,
+                          int64_t n_groups, int64_t n_vars, const double *clip, double *sum, double *sumsq,
+                          double *nnz) {
+    CREST_TRY(validate_chunk(chunk));
+    CREST_TRY(check_maps(chunk, n_vars));
+    CREST_REQUIRE(n_groups >= 0 && sum && (n_groups * n_vars == 0 || group_of_row), CREST_EINVAL,
+                  "sum, sumsq, nnz must be (n_groups, n_vars); group_of_row (n_rows,)");
+    int64_t n_rows = 0;
+    for (int64_t i = 0; i < chunk->n_cell_map; ++i) n_rows = std::max<int64_t>(n_rows, chunk->cell_map[i] + 1);
+    CREST_REQUIRE(n_group_rows >= n_rows, CREST_EINVAL,
+                  "sum, sumsq, nnz must be (n_groups, n_vars); group_of_row (n_rows,)");
+    for (int64_t r = 0; r < n_group_rows; ++r)
+        CREST_REQUIRE(group_of_row[r] == 0xffffffffu || (int64_t)group_of_row[r] < n_groups, CREST_EINVAL,
+                      "group id out of range");
+    Ctx *x;
+    CREST_TRY(get_ctx(&x));
+    std::lock_guard<std::mutex> lock(x->mu);
+    HostSpans s;
+    make_spans(chunk, s);
+    DevChunk dc;
+    CREST_TRY(stage_chunk(*x, chunk, s, dc));
+    cudaStream_t st = x->st;
+    const int64_t ne = n_groups * n_vars;
+    CREST_TRY(upload(x->out5, group_of_row, n_group_rows, st));
+    const double *dclip = nullptr;
+    if (clip) {
+        CREST_TRY(upload(x->out4, clip, ne, st));
+        dclip = x->out4.as<double>();
+    }
+    CREST_TRY(zeros<double>(x->out0, ne, st));
+    if (sumsq) CREST_TRY(zeros<double>(x->out1, ne, st));
+    if (nnz) CREST_TRY(zeros<double>(x->out2, ne, st));
+    CREST_TRY(launch_group_gene_sums(dc, x->out5.as<uint32_t>(), n_vars, dclip, x->out0.as<double>(),
+                                     sumsq ? x->out1.as<double>() : nullptr, nnz ? x->out2.as<double>() : nullptr,
+                                     st));
+    std::vector<double> h0(ne), h1(sumsq ? ne : 0), h2(nnz ? ne : 0);
+    if (ne) {
+        CREST_CUDA_TRY(cudaMemcpyAsync(h0.data(), x->out0.ptr, 8 * ne, cudaMemcpyDeviceToHost, st));
+        if (sumsq) CREST_CUDA_TRY(cudaMemcpyAsync(h1.data(), x->out1.ptr, 8 * ne, cudaMemcpyDeviceToHost, st));
+        if (nnz) CREST_CUDA_TRY(cudaMemcpyAsync(h2.data(), x->out2.ptr, 8 * ne, cudaMemcpyDeviceToHost, st));
+    }
+    CREST_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int64_t i = 0; i < ne; ++i) sum[i] += h0[i];
+    for (int64_t i = 0; sumsq && i < ne; ++i) sumsq[i] += h1[i];
+    for (int64_t i = 0; nnz && i < ne; ++i) nnz[i] += h2[i];
+    return CREST_OK;
+}
+
+int crest_group_gene_totals(const crest_chunk *chunk, const uint32_t *group_of_row, int64_t n_group_rows,
+                            int64_t n_groups, int64_t n_vars, double *sum) {
+    return crest_group_gene_sums(chunk, group_of_row, n_group_rows, n_groups, n_vars, nullptr, sum, nullptr,
+                                 nullptr);
 }
 
 int crest_project(const crest_chunk *chunk, const int32_t *sub_map, int64_t n_vars, const double *loadings,

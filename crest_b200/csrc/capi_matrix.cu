@@ -505,6 +505,49 @@ int crest_matrix_gene_stats(crest_matrix *m, const int64_t *cell_map, const int3
     return CREST_OK;
 }
 
+int crest_matrix_group_gene_sums(crest_matrix *m, const int64_t *cell_map, const int32_t *gene_map, double target_sum,
+                                 int32_t log1p, const uint32_t *group_of_row, int64_t n_group_rows, int64_t n_groups,
+                                 int64_t n_vars, const double *clip, double *sum, double *sumsq, double *nnz) {
+    CREST_REQUIRE(m && sum && n_groups >= 0, CREST_EINVAL, "NULL argument");
+    CREST_TRY(bind_device(m->device));
+    int64_t n_rows = 0;
+    for (int64_t i = 0; i < m->n_cells; ++i) n_rows = std::max<int64_t>(n_rows, cell_map[i] + 1);
+    CREST_REQUIRE(n_group_rows >= n_rows && (n_group_rows == 0 || group_of_row), CREST_EINVAL,
+                  "sum, sumsq, nnz must be (n_groups, n_vars); group_of_row (n_rows,)");
+    for (int64_t r = 0; r < n_group_rows; ++r)
+        CREST_REQUIRE(group_of_row[r] == 0xffffffffu || (int64_t)group_of_row[r] < n_groups, CREST_EINVAL,
+                      "group id out of range");
+    CREST_TRY(stage_maps(m, cell_map, gene_map, -1, n_vars));
+    cudaStream_t st = m->compute;
+    const int64_t ne = n_groups * n_vars;
+    CREST_TRY(upload(m->out[3], group_of_row, n_group_rows, st));
+    const double *dclip = nullptr;
+    if (clip) {
+        CREST_TRY(upload(m->out[4], clip, ne, st));
+        dclip = m->out[4].as<double>();
+    }
+    CREST_TRY(zeros<double>(m->out[0], ne, st));
+    if (sumsq) CREST_TRY(zeros<double>(m->out[1], ne, st));
+    if (nnz) CREST_TRY(zeros<double>(m->out[2], ne, st));
+    const DevChunk proto = base_chunk(m, target_sum, log1p);
+    CREST_TRY(for_each_piece(m, proto, m->n_cells, [&](const DevChunk &c) {
+        return launch_group_gene_sums(c, m->out[3].as<uint32_t>(), n_vars, dclip, m->out[0].as<double>(),
+                                      sumsq ? m->out[1].as<double>() : nullptr, nnz ? m->out[2].as<double>() : nullptr,
+                                      st);
+    }));
+    std::vector<double> h0(ne), h1(sumsq ? ne : 0), h2(nnz ? ne : 0);
+    if (ne) {
+        CREST_CUDA_TRY(cudaMemcpyAsync(h0.data(), m->out[0].ptr, 8 * ne, cudaMemcpyDeviceToHost, st));
+        if (sumsq) CREST_CUDA_TRY(cudaMemcpyAsync(h1.data(), m->out[1].ptr, 8 * ne, cudaMemcpyDeviceToHost, st));
+        if (nnz) CREST_CUDA_TRY(cudaMemcpyAsync(h2.data(), m->out[2].ptr, 8 * ne, cudaMemcpyDeviceToHost, st));
+    }
+    CREST_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int64_t i = 0; i < ne; ++i) sum[i] += h0[i];
+    for (int64_t i = 0; sumsq && i < ne; ++i) sumsq[i] += h1[i];
+    for (int64_t i = 0; nnz && i < ne; ++i) nnz[i] += h2[i];
+    return CREST_OK;
+}
+
 int crest_pca_create(crest_pca **out, int64_t d, int32_t precision) {
     CREST_REQUIRE(out, CREST_EINVAL, "out is NULL");
     *out = nullptr;

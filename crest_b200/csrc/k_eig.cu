@@ -25,6 +25,7 @@
 //    Ritz uses the same Jacobi kernel on the p x p projected matrix.
 // Stops when every wanted residual ||C v - theta v|| <= tol * theta_1.
 #include <math.h>
+#include <stdlib.h>
 
 #include <algorithm>
 #include <mutex>
@@ -301,8 +302,7 @@ __global__ void __launch_bounds__(512) k_jacobi(const double *__restrict__ Ain, 
     int sweep = 0;
     for (; sweep < max_sweeps; ++sweep) {
         for (int r = 0; r < n - 1; ++r) {
-            if (tid < half) {
-                const int i = tid;
+            for (int i = tid; i < half; i += nt) {
                 const int a = (i == 0) ? 0 : ((i - 1 + r) % (n - 1)) + 1;
                 const int b = ((n - 2 - i + r) % (n - 1)) + 1;
                 const int p = a < b ? a : b, q = a < b ? b : a;
@@ -388,18 +388,27 @@ __global__ void __launch_bounds__(512) k_jacobi(const double *__restrict__ Ain, 
 
 // V: n_in x n_in eigenvectors (col-major); Vwork: (n_in+1)^2 doubles of
 // global scratch, used when the rotations do not fit in shared memory.
+// Threads of the Jacobi CTA (CREST_JACOBI_THREADS, a multiple of 32 in [64, 512]).
+static int jacobi_threads() {
+    const char *e = getenv("CREST_JACOBI_THREADS");
+    int v = e ? atoi(e) : 512;
+    v = (v / 32) * 32;
+    return v < 64 ? 64 : (v > 512 ? 512 : v);
+}
+
 int jacobi(const double *A, int n_in, double *Vwork, double *V, double *vals, int *sweeps, cudaStream_t st) {
     const int n = n_in + (n_in & 1);
     CREST_REQUIRE(n <= kJacobiMax, CREST_EINVAL, "Jacobi size %d exceeds %d", n, kJacobiMax);
     prof::Scope ps("eig_jacobi", st);
+    const int nt = jacobi_threads();
     if (n <= kJacobiSmemV) {
         const size_t smem = sizeof(double) * ((size_t)n * (n + 1) + (size_t)n * n);
         CREST_TRY(ensure_smem_attr((const void *)k_jacobi<true>, (size_t)smem));
-        k_jacobi<true><<<1, 512, smem, st>>>(A, n_in, n, nullptr, V, vals, 40, sweeps);
+        k_jacobi<true><<<1, nt, smem, st>>>(A, n_in, n, nullptr, V, vals, 40, sweeps);
     } else {
         const size_t smem = sizeof(double) * (size_t)n * (size_t)(n + 1);
         CREST_TRY(ensure_smem_attr((const void *)k_jacobi<false>, (size_t)smem));
-        k_jacobi<false><<<1, 512, smem, st>>>(A, n_in, n, Vwork, V, vals, 40, sweeps);
+        k_jacobi<false><<<1, nt, smem, st>>>(A, n_in, n, Vwork, V, vals, 40, sweeps);
     }
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;

@@ -47,7 +47,7 @@ constexpr int kStageBytes = 4 * kOperandBytes;          // A_hi, A_lo, B_hi, B_l
 constexpr int kEpiWarps = 8;      // 2 per TMEM lane quadrant, 64 accumulator columns each
 constexpr int kThreads = (2 + kEpiWarps) * 32;
 constexpr uint32_t kTmemCols = 512;
-constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s
+constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s: the limit of every pipeline wait
 
 // instruction descriptor, kind::f16: D f32 (bit 4), A bf16 (bits 7-9 = 1),
 // B bf16 (bits 10-12 = 1), A and B MN-major (bits 15, 16), N>>3 at bit 17,
@@ -92,16 +92,18 @@ __device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait: false (and an error code in *err) after kWaitNs.  The error
-// word (global memory) is only looked at on the slow path, every 64 polls,
-// so another role's failure also ends this wait.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
+// Bounded wait: false (and an error code in *err) after `limit` ns (kWaitNs
+// unless a test shortens it).  The error word (global memory) is only looked
+// at on the slow path, every 64 polls, so another role's failure also ends
+// this wait.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, int code,
+                                          unsigned long long limit) {
     if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = globaltimer();
     for (uint32_t n = 1;; ++n) {
         if (mbar_try(bar, parity)) return true;
         if ((n & 63u) == 0) {
-            if (globaltimer() - t0 > kWaitNs) {
+            if (globaltimer() - t0 > limit) {
                 atomicCAS(err, 0, code);
                 return false;
             }
@@ -177,13 +179,16 @@ struct TcArgs {
     const int64_t *n_kept;
     double *G;             // [d x d]
     int *err;
+    unsigned long long wait_ns;  // limit of every pipeline wait
+    int stall_stage;       // test hook: the producer leaves this stage's loads out (-1: none)
 };
 
 // Bounded mbarrier wait made by lane 0 and broadcast, so the calling warp
 // stays converged (the .sync.aligned tcgen05 instructions need the whole warp).
-__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
+__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, int *err, int code,
+                                          unsigned long long limit) {
     int got = 0;
-    if ((threadIdx.x & 31) == 0) got = mbar_wait(bar, parity, err, code) ? 1 : 0;
+    if ((threadIdx.x & 31) == 0) got = mbar_wait(bar, parity, err, code, limit) ? 1 : 0;
     return __shfl_sync(0xffffffffu, got, 0) != 0;
 }
 
@@ -195,7 +200,7 @@ __device__ __forceinline__ void tc_epilogue(const TcArgs &a, int bi, int bj, uin
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int &epi_ok = *epi_ok_sh;
     auto warp_wait = [&](uint64_t *bar, uint32_t parity, int code) -> bool {
-        return ::crest::warp_wait(bar, parity, a.err, code);
+        return ::crest::warp_wait(bar, parity, a.err, code, a.wait_ns);
     };
     const int q = warp & 3;              // TMEM lane quadrant this warp may access
     const int h = (warp - 2) >> 2;       // column group: 64 h .. 64 h + 63
@@ -294,7 +299,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_bf16x3(const __grid_consta
     // converged (the .sync.aligned tcgen05 instructions need the whole warp).
     auto warp_wait = [&](uint64_t *bar, uint32_t parity, int code) -> bool {
         int got = 0;
-        if (lane == 0) got = mbar_wait(bar, parity, a.err, code) ? 1 : 0;
+        if (lane == 0) got = mbar_wait(bar, parity, a.err, code, a.wait_ns) ? 1 : 0;
         return __shfl_sync(0xffffffffu, got, 0) != 0;
     };
     const int n_periods = (a.n_stages + a.fold - 1) / a.fold;
@@ -307,7 +312,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_bf16x3(const __grid_consta
         for (int i = 0; i < a.n_stages; ++i) {
             const int s = i % kStages;
             if (i >= kStages && !warp_wait(&empty_bar[s], ((i / kStages) - 1) & 1, 1)) break;
-            if (lane == 0) {
+            if (lane == 0 && i == a.stall_stage) {
+                mbar_expect_tx(&full_bar[s], bytes);  // armed, never filled: the consumer's wait runs out
+            } else if (lane == 0) {
                 uint8_t *st = ring + (size_t)s * kStageBytes;
                 mbar_expect_tx(&full_bar[s], bytes);
                 const int y = i * kStageCells;  // first cell of the stage
@@ -440,13 +447,13 @@ __device__ __forceinline__ bool try_cluster(uint64_t *bar, uint32_t parity) {
 }
 
 // Bounded wait (as mbar_wait) with cluster-scope acquire.
-__device__ __forceinline__ bool wait(uint64_t *bar, uint32_t parity, int *err, int code) {
+__device__ __forceinline__ bool wait(uint64_t *bar, uint32_t parity, int *err, int code, unsigned long long limit) {
     if (try_cluster(bar, parity)) return true;
     const unsigned long long t0 = globaltimer();
     for (uint32_t n = 1;; ++n) {
         if (try_cluster(bar, parity)) return true;
         if ((n & 63u) == 0) {
-            if (globaltimer() - t0 > kWaitNs) {
+            if (globaltimer() - t0 > limit) {
                 atomicCAS(err, 0, code);
                 return false;
             }
@@ -455,9 +462,10 @@ __device__ __forceinline__ bool wait(uint64_t *bar, uint32_t parity, int *err, i
     }
 }
 
-__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, int *err, int code) {
+__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, int *err, int code,
+                                          unsigned long long limit) {
     int got = 0;
-    if ((threadIdx.x & 31) == 0) got = wait(bar, parity, err, code) ? 1 : 0;
+    if ((threadIdx.x & 31) == 0) got = wait(bar, parity, err, code, limit) ? 1 : 0;
     return __shfl_sync(0xffffffffu, got, 0) != 0;
 }
 
@@ -503,6 +511,8 @@ struct Args {
     const int64_t *n_kept;
     double *G, *G_aux;     // [d x d]: cell halves 0 and 1
     int *err;
+    unsigned long long wait_ns;  // limit of every pipeline wait
+    int stall_stage;       // test hook: the leader's producer leaves this stage out (-1: none)
 };
 
 __global__ void __launch_bounds__(kThreads, 1) k_syrk_pair(const __grid_constant__ CUtensorMap tmap, Args a) {
@@ -552,8 +562,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_pair(const __grid_constant
         int issued = 0;
         for (int i = 0; i < n_my; ++i) {
             const int s = i % kStages;
-            if (i >= kStages && !warp_wait(&empty_bar[s], ((i / kStages) - 1) & 1, a.err, 11)) break;
-            if (lane == 0) {
+            if (i >= kStages && !warp_wait(&empty_bar[s], ((i / kStages) - 1) & 1, a.err, 11, a.wait_ns)) break;
+            if (lane == 0 && leader && i == a.stall_stage) {
+                mbar_expect_tx(&full_bar[s], 2 * bytes_cta);  // armed, never filled (test hook)
+            } else if (lane == 0) {
                 uint8_t *st = ring + (size_t)s * kStageBytes;
                 const uint32_t fb = mapa(smem_u32(&full_bar[s]), 0);
                 if (leader) mbar_expect_tx(&full_bar[s], 2 * bytes_cta);
@@ -574,19 +586,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_pair(const __grid_constant
         }
         // drain: the last stages' releases (MMA commits) land before exit
         for (int i = max(0, issued - kStages); i < issued; ++i)
-            if (!warp_wait(&empty_bar[i % kStages], (i / kStages) & 1, a.err, 15)) break;
+            if (!warp_wait(&empty_bar[i % kStages], (i / kStages) & 1, a.err, 15, a.wait_ns)) break;
     } else if (warp == 1) {
         // --------------------------------------------- MMA issuer (leader)
         if (leader) {
             bool ok = true;
             for (int p = 0; p < n_periods && ok; ++p) {
                 const int buf = p % kAccBufs;
-                if (p >= kAccBufs && !warp_wait(&acc_empty[buf], ((p / kAccBufs) - 1) & 1, a.err, 12)) break;
+                if (p >= kAccBufs && !warp_wait(&acc_empty[buf], ((p / kAccBufs) - 1) & 1, a.err, 12, a.wait_ns)) break;
                 const uint32_t d_tmem = tmem + (uint32_t)(buf * kAccCols);
                 const int i0 = p * a.fold, i1 = min(n_my, i0 + a.fold);
                 for (int i = i0; i < i1; ++i) {
                     const int s = i % kStages;
-                    if (!warp_wait(&full_bar[s], (i / kStages) & 1, a.err, 13)) {
+                    if (!warp_wait(&full_bar[s], (i / kStages) & 1, a.err, 13, a.wait_ns)) {
                         ok = false;
                         break;
                     }
@@ -624,7 +636,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_pair(const __grid_constant
         const uint32_t empty_leader[2] = {mapa(smem_u32(&acc_empty[0]), 0), mapa(smem_u32(&acc_empty[1]), 0)};
         for (int p = 0; p < n_periods; ++p) {
             const int buf = p % kAccBufs;
-            if (!warp_wait(&acc_full[buf], (p / kAccBufs) & 1, a.err, 14)) {
+            if (!warp_wait(&acc_full[buf], (p / kAccBufs) & 1, a.err, 14, a.wait_ns)) {
                 ok = false;
                 break;
             }
@@ -706,6 +718,18 @@ static ErrFlag g_tc_err[64];
 // default 128 cells; at 1M cells periods of 64, 128 and 256 cells all keep
 // the top-50 subspace within 0.007 degree of the FP64 Gram, 512 cells drift
 // past 0.01 degree).
+// Failure-injection hook for tests (host side, read at every launch):
+// CREST_TC_INJECT_STALL=1 makes the producer arm the last stage of the launch
+// without loading it and shortens every pipeline wait to 5 ms, so the MMA
+// issuer's wait runs out, the kernel records the error and returns with its
+// TMEM released; the next call reports CREST_ETIMEOUT.  Off by default.
+void tc_test_hooks(int n_stages, unsigned long long &wait_ns, int &stall_stage) {
+    const char *e = getenv("CREST_TC_INJECT_STALL");
+    const bool on = e && e[0] == '1' && n_stages > 0;
+    wait_ns = on ? 5000000ull : kWaitNs;
+    stall_stage = on ? n_stages - 1 : -1;
+}
+
 // CTA-pair SYRK (default) or one CTA per 128 x 128 block (CREST_TC_PAIR=0).
 bool tc_pair_enabled() {
     const char *e = getenv("CREST_TC_PAIR");
@@ -771,6 +795,7 @@ int syrk_bf16x3_fold(const GramWork &w, int64_t m_pad, const DevScale &t, double
     a.n_kept = w.n_kept;
     a.G = gram;
     a.err = err;
+    tc_test_hooks(a.n_stages, a.wait_ns, a.stall_stage);
     if (tc_pair_enabled() && w.gram_aux && w.d_pad % pair::kN == 0) {
         pair::Args b;
         b.d = w.d;
@@ -785,6 +810,8 @@ int syrk_bf16x3_fold(const GramWork &w, int64_t m_pad, const DevScale &t, double
         b.G = gram;
         b.G_aux = w.gram_aux;
         b.err = err;
+        b.wait_ns = a.wait_ns;
+        b.stall_stage = a.stall_stage < 0 ? -1 : (a.stall_stage - a.n_stages / 2);  // in the second cell half
         const size_t smem = 1024 + (size_t)kStages * pair::kStageBytes;
         prof::Scope ps("syrk_bf16x3_tcgen05_pair", st);
         CREST_TRY(ensure_smem_attr((const void *)pair::k_syrk_pair, smem));

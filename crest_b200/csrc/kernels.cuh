@@ -25,6 +25,9 @@ struct RowOut {  // per-row QC results added at the cell's row (matrix API)
 int launch_qc(const DevChunk &c, const uint8_t *flag, uint32_t *gene_ncells, double *gene_total,
               const SpanOut *span, const RowOut *row, cudaStream_t st);
 int launch_gene_stats(const DevChunk &c, double *out, cudaStream_t st);
+// Per (group, var) sums of the transformed values (sumsq / nnz / clip may be NULL).
+int launch_group_gene_sums(const DevChunk &c, const uint32_t *group_of_row, int64_t n_vars, const double *clip,
+                           double *sum, double *sumsq, double *nnz, cudaStream_t st);
 // Gene-range index of a device-resident CSR matrix with rows sorted by gene
 // id: off[cell * (n_ranges - 1) + b - 1] = first entry of the row (relative
 // to its start) with gene >= b << log2_s, b = 1 .. n_ranges - 1.

@@ -21,7 +21,7 @@ from . import _lib, _native, dist
 from .core import BioFrame
 
 __all__ = ["calculate_qc_metrics", "filter_cells", "filter_genes", "normalize_total", "log1p", "scale",
-           "gene_stats", "highly_variable_genes", "hvg_from_stats"]
+           "gene_stats", "group_gene_sums", "highly_variable_genes", "hvg_from_stats"]
 
 
 # --------------------------------------------------------------------------- QC
@@ -143,6 +143,39 @@ def gene_stats(bf: BioFrame) -> np.ndarray:
         for ctx in bf.iter_ctx():
             _native.gene_stats(*ctx, out)
     return dist.sum_host(out)
+
+
+def group_gene_sums(bf: BioFrame, group_of_row: np.ndarray, n_groups: int, clip: Optional[np.ndarray] = None,
+                    transform: bool = True, stats: bool = True):
+    """Per (group, gene) sum, sum of squares and non-zero count of the (lazily
+    transformed, unless ``transform`` is False) matrix, each (n_groups, n_vars);
+    ``group_of_row`` gives each cell's group (0xffffffff: none) and ``clip``
+    (n_groups, n_vars) caps values first.  With ``stats=False`` only the sums."""
+    G, V = int(n_groups), bf.n_vars
+    grp = np.ascontiguousarray(group_of_row, dtype=np.uint32)
+    if len(grp) != bf.n_obs:
+        raise ValueError("group_of_row must have one entry per cell")
+    if bool(np.any((grp != np.iinfo(np.uint32).max) & (grp >= G))):
+        raise ValueError("group id out of range")
+    s = np.zeros((G, V))
+    q = np.zeros((G, V)) if stats else None
+    z = np.zeros((G, V)) if stats else None
+    c = None if clip is None else np.ascontiguousarray(clip, dtype=np.float64)
+    if c is not None and c.shape != (G, V):
+        raise ValueError("clip must be (n_groups, n_vars)")
+    dm = bf.device_matrix()
+    if dm is not None:
+        cmap, gmap = bf._cell_map(), bf._gene_map()
+        target, log = bf._transform() if transform else (0.0, False)
+        _lib.call("crest_matrix_group_gene_sums", dm.handle, _lib.ptr(cmap), _lib.ptr(gmap), float(target), int(log),
+                  _lib.ptr(grp), len(grp), G, V, _lib.ptr(c), _lib.ptr(s), _lib.ptr(q), _lib.ptr(z))
+    else:
+        for ctx in bf.iter_ctx(transform=transform):
+            if stats:
+                _native.group_gene_sums(*ctx, grp, s, q, z, c)
+            else:
+                _native.group_gene_totals(*ctx, grp, s)
+    return (s, q, z) if stats else s
 
 
 def _mean_var(s1: np.ndarray, s2: np.ndarray, n: int):

@@ -11,7 +11,7 @@ import numpy as np
 
 from . import _lib, _native, dist
 from .core import BioFrame
-from .pp import _mean_var, gene_stats
+from .pp import _mean_var, gene_stats, group_gene_sums
 
 __all__ = ["pca"]
 
@@ -104,7 +104,8 @@ class PcaPlan:
 def pca(bf: BioFrame, n_comps: int = 50, use_highly_variable: Optional[bool] = None,
         scale: Optional[bool] = None, max_value: Optional[float] = None,
         gram_precision: str = "bf16x3") -> BioFrame:
-    """Exact PCA of the (optionally scaled) matrix via its covariance, streamed.
+    """Principal components of the selected genes from their covariance, without
+    ever materialising the dense (scaled) matrix.
 
     One pass accumulates the gene x gene Gram matrix of the selected genes
     (``gram_precision``: "bf16x3" split-BF16 tensor-core products, "fp32" plain
@@ -182,3 +183,76 @@ def pca(bf: BioFrame, n_comps: int = 50, use_highly_variable: Optional[bool] = N
     if stats is not None:
         bf.uns["pca"]["timings"] = stats
     return bf
+
+
+# --------------------------------------------------------------------------- differential expression
+def _natural_key(label: str):
+    """Sort key putting "2" before "10" (digits compared as numbers)."""
+    import re
+    return [int(t) if t.isdigit() else t for t in re.split(r"(\d+)", label)]
+
+
+def _bh(p: np.ndarray) -> np.ndarray:
+    """Benjamini-Hochberg adjusted p-values (step-up, capped at 1)."""
+    n = len(p)
+    order = np.argsort(p)
+    scaled = p[order] * n / np.arange(1, n + 1)
+    adj = np.minimum.accumulate(scaled[::-1])[::-1]
+    out = np.empty(n)
+    out[order] = np.minimum(adj, 1.0)
+    return out
+
+
+def rank_genes_groups(bf: BioFrame, groupby: str, method: str = "t-test", groups="all",
+                      n_genes: Optional[int] = 100):
+    """Each group against all other cells with a Welch t-test on the (lazily
+    normalised / log-transformed) matrix, as the reference's
+    ``crest.tl.rank_genes_groups(method="t-test")`` (crest/tl.py:205-288): the
+    per (group, gene) sums come from one GPU pass (group_gene_sums); means,
+    variances, Welch's statistic and degrees of freedom, log fold changes, p-values
+    and Benjamini-Hochberg adjustment are O(groups x genes) host arithmetic.
+    Returns a long DataFrame (group, names, scores, logfoldchanges, pvals,
+    pvals_adj) with the top ``n_genes`` genes per group by score, also kept in
+    ``uns['rank_genes_groups']``."""
+    import pandas as pd
+    if method != "t-test":
+        raise NotImplementedError("only method='t-test' is provided (the Wilcoxon rank test is not on this path)")
+    labels = bf.obs[groupby].astype(str).where(bf.obs[groupby].notna(), None).to_numpy()
+    cats = sorted({x for x in labels if x is not None}, key=_natural_key)
+    if groups != "all":
+        keep = set(groups)
+        cats = [c for c in cats if c in keep]
+    index = {c: i for i, c in enumerate(cats)}
+    none = np.iinfo(np.uint32).max
+    grp = np.array([index.get(x, none) if x is not None else none for x in labels], dtype=np.uint32)
+    G = len(cats)
+    sizes = np.bincount(grp[grp != none], minlength=G).astype(np.float64)
+    N = sizes.sum()
+    s, q, _ = group_gene_sums(bf, grp, G)
+    s_all, q_all = s.sum(0), q.sum(0)
+    names = np.array(bf.var_names, dtype=object)
+    k = bf.n_vars if n_genes is None else min(n_genes, bf.n_vars)
+    frames = []
+    for i, c in enumerate(cats):
+        n1, n2 = sizes[i], N - sizes[i]
+        m1 = s[i] / n1
+        m2 = (s_all - s[i]) / n2
+        lfc = np.log2((np.expm1(m1) + 1e-9) / (np.expm1(m2) + 1e-9))
+        v1 = np.maximum((q[i] - n1 * m1 ** 2) / (n1 - 1), 0)
+        v2 = np.maximum(((q_all - q[i]) - n2 * m2 ** 2) / (n2 - 1), 0)
+        a, b = v1 / n1, v2 / n2
+        with np.errstate(divide="ignore", invalid="ignore"):
+            t = (m1 - m2) / np.sqrt(a + b)
+            df = (a + b) ** 2 / (a ** 2 / (n1 - 1) + b ** 2 / (n2 - 1))
+        df = np.where(np.isnan(df), 1.0, df)
+        pv = _native.t_pvalues(t, df)
+        t = np.where(np.isnan(t), 0.0, t)
+        pv = np.where(np.isnan(pv), 1.0, pv)
+        padj = _bh(pv)
+        top = np.argsort(-t, kind="stable")[:k]
+        frames.append(pd.DataFrame({"group": [c] * k, "names": names[top].astype(str), "scores": t[top],
+                                    "logfoldchanges": lfc[top], "pvals": pv[top], "pvals_adj": padj[top]}))
+    out = pd.concat(frames, ignore_index=True) if frames else pd.DataFrame()
+    bf.uns["rank_genes_groups"] = {"params": {"groupby": groupby, "method": method, "reference": "rest"},
+                                   "groups": cats, "table": out}
+    return out

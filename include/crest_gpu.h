@@ -115,6 +115,19 @@ int crest_qc(const crest_chunk *chunk, const uint8_t *flag, int64_t n_vars, doub
              uint32_t *cell_ngenes, double *cell_flag, int64_t n_rows, uint32_t *gene_ncells,
              double *gene_total);
 
+/* group_gene_sums: src/py.rs:311-338, src/kernels.rs:388-442.  Per (group,
+ * var) sum, sum of squares and count of the transformed stored values of
+ * kept cells; group_of_row[row] is the group of a cell's row (0xffffffff: no
+ * group), n_group_rows >= n_rows; clip (n_groups x n_vars, may be NULL) caps
+ * each value first.  sum / sumsq / nnz are (n_groups x n_vars) row-major and
+ * accumulated; sumsq and nnz may be NULL. */
+int crest_group_gene_sums(const crest_chunk *chunk, const uint32_t *group_of_row, int64_t n_group_rows,
+                          int64_t n_groups, int64_t n_vars, const double *clip, double *sum, double *sumsq,
+                          double *nnz);
+/* group_gene_totals: src/py.rs:340-357 (pseudobulk sums only). */
+int crest_group_gene_totals(const crest_chunk *chunk, const uint32_t *group_of_row, int64_t n_group_rows,
+                            int64_t n_groups, int64_t n_vars, double *sum);
+
 /* crest_qc_static: no counterpart in the reference.  Same arguments and
  * results as crest_qc, computed without allocating device memory: the
  * kernel runs on a fixed scratch array compiled into the library (about
@@ -180,6 +193,12 @@ int crest_matrix_qc(crest_matrix *m, const int64_t *cell_map, const int32_t *gen
 /* Whole-matrix gene_stats pass (crest/pp.py:115-120).  out (n_vars, 5). */
 int crest_matrix_gene_stats(crest_matrix *m, const int64_t *cell_map, const int32_t *gene_map,
                             double target_sum, int32_t log1p, int64_t n_vars, double *out);
+
+/* group_gene_sums over a whole matrix (same arguments and results as
+ * crest_group_gene_sums, with the matrix's cell_map / gene_map). */
+int crest_matrix_group_gene_sums(crest_matrix *m, const int64_t *cell_map, const int32_t *gene_map, double target_sum,
+                                 int32_t log1p, const uint32_t *group_of_row, int64_t n_group_rows, int64_t n_groups,
+                                 int64_t n_vars, const double *clip, double *sum, double *sumsq, double *nnz);
 
 /* PCA plan (crest/tl.py:37-91): Gram pass, centring + eigensolve, projection. */
 int crest_pca_create(crest_pca **out, int64_t d, int32_t precision);

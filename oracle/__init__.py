@@ -72,6 +72,7 @@ def lib():
         L.oc_materialize.argtypes = [P, C.c_int, P, P, P, C.c_int64]
         L.oc_materialize.restype = C.c_int64
         L.oc_synth.argtypes = [P, P, P, P, P, C.c_int]
+        L.oc_group_gene_sums.argtypes = [P, P, C.c_int64, P, P, P, P]
         _lib = L
     return _lib
 
@@ -205,6 +206,49 @@ def materialize(genes, values, cell_map, gene_map, target_sum, log1p, cells, ind
     r, g, x = np.empty(cap, np.uint32), np.empty(cap, np.uint32), np.empty(cap, np.float32)
     n = lib().oc_materialize(C.byref(ch), 1, _ptr(r), _ptr(g), _ptr(x), cap)
     return r[:n].copy(), g[:n].copy(), x[:n].copy()
+
+
+def group_gene_sums(genes, values, cell_map, gene_map, target_sum, log1p, cells, indptr, first_cell,
+                    group_of_row, sum, sumsq, nnz, clip=None):
+    """src/py.rs:311-338 / src/kernels.rs:388-442."""
+    ch, keep, nr = _view(genes, values, cell_map, gene_map, target_sum, log1p, cells, indptr, first_cell)
+    nv = _n_var(gene_map)
+    gr = _c(group_of_row, np.uint32, "group_of_row")
+    s, q, z = _c(sum, np.float64, "sum"), _c(sumsq, np.float64, "sumsq"), _c(nnz, np.float64, "nnz")
+    if s.ndim != 2 or s.shape[1] != nv or q.shape != s.shape or z.shape != s.shape or len(gr) < nr:
+        raise ValueError("sum, sumsq, nnz must be (n_groups, n_vars); group_of_row (n_rows,)")
+    if np.any((gr != np.iinfo(np.uint32).max) & (gr >= s.shape[0])):
+        raise ValueError("group id out of range")
+    c = None if clip is None else _c(clip, np.float64, "clip")
+    if c is not None and c.size != s.size:
+        raise ValueError("clip must be (n_groups, n_vars)")
+    lib().oc_group_gene_sums(C.byref(ch), _ptr(gr), nv, _ptr(c), _ptr(s), _ptr(q), _ptr(z))
+
+
+def group_gene_totals(genes, values, cell_map, gene_map, target_sum, log1p, cells, indptr, first_cell,
+                      group_of_row, sum):
+    """src/py.rs:340-357."""
+    ch, keep, nr = _view(genes, values, cell_map, gene_map, target_sum, log1p, cells, indptr, first_cell)
+    nv = _n_var(gene_map)
+    gr = _c(group_of_row, np.uint32, "group_of_row")
+    s = _c(sum, np.float64, "sum")
+    if s.ndim != 2 or s.shape[1] != nv or len(gr) < nr:
+        raise ValueError("sum must be (n_groups, n_vars); group_of_row (n_rows,)")
+    if np.any((gr != np.iinfo(np.uint32).max) & (gr >= s.shape[0])):
+        raise ValueError("group id out of range")
+    lib().oc_group_gene_sums(C.byref(ch), _ptr(gr), nv, None, _ptr(s), None, None)
+
+
+def t_pvalues(t, df):
+    """src/py.rs:413-427 (statrs StudentsT): 2 * sf(|t|, df) capped at 1, NaN for a
+    non-finite t or df <= 0; scipy's Student t here."""
+    from scipy import stats
+    t = np.asarray(t, np.float64)
+    df = np.asarray(df, np.float64)
+    ok = np.isfinite(t) & (df > 0)
+    p = np.full(t.shape, np.nan)
+    p[ok] = np.minimum(2.0 * stats.t.sf(np.abs(t[ok]), df[ok]), 1.0)
+    return p
 
 
 def pca_from_gram(gram, colsum, n, k):

@@ -518,3 +518,34 @@ int64_t oc_materialize(const oc_chunk *v, int n_threads, uint32_t *rows, uint32_
     free(bg); free(bx); free(sp);
     return n;
 }
+
+/* ------------------------------------------------------------------ group_gene_sums
+ * src/kernels.rs:388-442.  The reference materialises the chunk and lets
+ * each thread own a block of genes, walking the entries in order; every
+ * (group, gene) total is therefore an entry-order sum, which a sequential
+ * walk reproduces.  clip (n_groups x nv) may be NULL, sumsq / nnz too. */
+int oc_group_gene_sums(const oc_chunk *v, const uint32_t *group_of_row, int64_t nv, const double *clip, double *sum,
+                       double *sumsq, double *nnz) {
+    int64_t ns;
+    span_t *sp = cell_spans(v, &ns);
+    int64_t maxlen = max_span_len(sp, ns);
+    uint32_t *bg = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)maxlen);
+    float *bx = (float *)malloc(sizeof(float) * (size_t)maxlen);
+    for (int64_t i = 0; i < ns; i++) {
+        int64_t nb;
+        int64_t row = cell_entries(v, &sp[i], bg, bx, &nb);
+        if (row < 0) continue;
+        uint32_t grp = group_of_row[row];
+        if (grp == 0xffffffffu) continue;
+        for (int64_t e = 0; e < nb; e++) {
+            int64_t at = (int64_t)grp * nv + bg[e];
+            double x = (double)bx[e];
+            if (clip && clip[at] < x) x = clip[at];
+            sum[at] += x;
+            if (sumsq) sumsq[at] += x * x;
+            if (nnz) nnz[at] += 1.0;
+        }
+    }
+    free(bg); free(bx); free(sp);
+    return 0;
+}

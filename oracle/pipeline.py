@@ -315,3 +315,60 @@ def subspace_angles_deg(U, V):
     qb, _ = np.linalg.qr(np.asarray(V, np.float64))
     s = np.clip(np.linalg.svd(qa.T @ qb, compute_uv=False), -1.0, 1.0)
     return np.degrees(np.arccos(s))
+
+
+# --------------------------------------------------------------- crest/tl.py rank_genes_groups
+def rank_genes_groups(f: Frame, labels, n_genes=100):
+    """crest/tl.py:205-288, method "t-test": per (group, gene) sums over chunks
+    (group_gene_sums), then Welch's t, log fold change, p-values and BH per group.
+    ``labels`` holds one label (or None) per kept cell.  Returns a dict of columns."""
+    import re
+    from . import group_gene_sums, t_pvalues
+
+    def nat(s):
+        return [int(t) if t.isdigit() else t for t in re.split(r"(\d+)", s)]
+
+    labels = [None if x is None else str(x) for x in labels]
+    cats = sorted({x for x in labels if x is not None}, key=nat)
+    code = {c: i for i, c in enumerate(cats)}
+    none = np.iinfo(np.uint32).max
+    grp = np.array([code.get(x, none) if x is not None else none for x in labels], dtype=np.uint32)
+    G, V = len(cats), f.n_vars
+    sizes = np.bincount(grp[grp != none], minlength=G).astype(np.float64)
+    N = sizes.sum()
+    s, q, z = np.zeros((G, V)), np.zeros((G, V)), np.zeros((G, V))
+    for c in f.ctx():
+        group_gene_sums(*c, grp, s, q, z, None)
+    S_all, Q_all = s.sum(0), q.sum(0)
+    names = np.array(f.var_names(), dtype=object)
+    k = V if n_genes is None else min(n_genes, V)
+    cols = {"group": [], "names": [], "scores": [], "logfoldchanges": [], "pvals": [], "pvals_adj": []}
+    for i, cat in enumerate(cats):
+        n1, n2 = sizes[i], N - sizes[i]
+        m1 = s[i] / n1
+        m2 = (S_all - s[i]) / n2
+        logfc = np.log2((np.expm1(m1) + 1e-9) / (np.expm1(m2) + 1e-9))
+        v1 = np.maximum((q[i] - n1 * m1 ** 2) / (n1 - 1), 0)
+        v2 = np.maximum(((Q_all - q[i]) - n2 * m2 ** 2) / (n2 - 1), 0)
+        a, b = v1 / n1, v2 / n2
+        with np.errstate(divide="ignore", invalid="ignore"):
+            sc = (m1 - m2) / np.sqrt(a + b)
+            df = (a + b) ** 2 / (a ** 2 / (n1 - 1) + b ** 2 / (n2 - 1))
+        df = np.where(np.isnan(df), 1.0, df)
+        pv = t_pvalues(np.ascontiguousarray(sc), np.ascontiguousarray(df))
+        sc = np.where(np.isnan(sc), 0.0, sc)
+        pv = np.where(np.isnan(pv), 1.0, pv)
+        n = len(pv)
+        order = np.argsort(pv)
+        ranked = pv[order] * n / np.arange(1, n + 1)
+        adj = np.minimum.accumulate(ranked[::-1])[::-1]
+        padj = np.empty(n)
+        padj[order] = np.minimum(adj, 1.0)
+        top = np.argsort(-sc, kind="stable")[:k]
+        cols["group"] += [cat] * k
+        cols["names"] += list(names[top].astype(str))
+        cols["scores"] += list(sc[top])
+        cols["logfoldchanges"] += list(logfc[top])
+        cols["pvals"] += list(pv[top])
+        cols["pvals_adj"] += list(padj[top])
+    return {key: np.asarray(v) for key, v in cols.items()}

@@ -30,6 +30,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 REF = None  # the reference checkout, from the command line
 OUT = os.path.dirname(os.path.abspath(__file__))
 THREADS = 4  # rayon thread count emulated by the oracle (fixes the per-gene sum order)
+DE_TOP = 25  # genes per group kept in the differential-expression fixture
 
 
 # ------------------------------------------------------------------ fake polars
@@ -115,9 +116,15 @@ class DataFrame:
         return d
 
 
+def concat(frames):
+    d = DataFrame()
+    d.cols = {k: np.concatenate([f.cols[k] for f in frames]) for k in frames[0].cols} if frames else {}
+    return d
+
+
 def install_fakes():
     pl = types.ModuleType("polars")
-    pl.Series, pl.DataFrame = Series, DataFrame
+    pl.Series, pl.DataFrame, pl.concat = Series, DataFrame, concat
     pl.Utf8, pl.UInt32, pl.Float32, pl.Int64 = "utf8", "u32", "f32", "i64"
     sys.modules["polars"] = pl
     sys.path.insert(0, ROOT)
@@ -132,7 +139,7 @@ def install_fakes():
 
 
 def run_reference(crest, indptr, indices, data, n_genes, names, n_top, n_comps, min_genes, min_cells,
-                  chunk_nnz=None):
+                  chunk_nnz=None, labels=None):
     bf = crest.BioFrame.from_csr(indptr, indices, data, n_genes, var=DataFrame({"gene_name": np.array(names)}))
     if chunk_nnz:
         bf.chunk_nnz = chunk_nnz
@@ -144,7 +151,16 @@ def run_reference(crest, indptr, indices, data, n_genes, names, n_top, n_comps, 
     crest.pp.highly_variable_genes(bf, n_top_genes=n_top)
     crest.pp.scale(bf, max_value=10)
     crest.tl.pca(bf, n_comps=n_comps)
-    return {
+    de = {}
+    if labels is not None:  # differential expression of the synthetic clusters (t-test, each vs rest)
+        kept = bf.obs["cell_id"].to_numpy().astype(np.int64)
+        bf.obs = bf.obs.with_columns(Series("cluster", np.array([f"c{x}" for x in labels[kept]])))
+        tab = crest.tl.rank_genes_groups(bf, "cluster", method="t-test", n_genes=DE_TOP)
+        de = {f"de_{k}": tab[k].to_numpy() for k in ("group", "names", "scores", "logfoldchanges", "pvals",
+                                                      "pvals_adj")}
+        de["de_group"] = de["de_group"].astype(str)
+        de["de_names"] = de["de_names"].astype(str)
+    return {**de,
         "qc_n_genes_by_counts": obs0["n_genes_by_counts"].to_numpy().astype(np.int64),
         "qc_total_counts": obs0["total_counts"].to_numpy(),
         "qc_pct_counts_mt": obs0["pct_counts_mt"].to_numpy(),
@@ -175,6 +191,16 @@ CASES = {
 }
 
 
+def case_labels(name):
+    """Cluster label of every input cell (the generator's own assignment)."""
+    sys.path.insert(0, ROOT)
+    from crest_b200 import synth
+    c = CASES[name]
+    if c["kind"] == "params":
+        return synth.make_params(*c["args"]).labels
+    return synth.workload_params(synth.WORKLOADS[c["name"]]).labels
+
+
 def case_input(name):
     sys.path.insert(0, ROOT)
     from crest_b200 import synth
@@ -196,7 +222,7 @@ def main():
     for name, c in CASES.items():
         indptr, indices, data, n_genes, names = case_input(name)
         res = run_reference(crest, indptr, indices, data, n_genes, names, c["n_top"], c["n_comps"], c["min_genes"],
-                            c["min_cells"])
+                            c["min_cells"], labels=case_labels(name))
         if name != "small":  # keep the committed fixture small
             res["X_pca"] = res["X_pca"][:256]
             res["PCs"] = res["PCs"][res["highly_variable"]][:, :10]

@@ -112,3 +112,91 @@ def test_sums_are_the_identity_without_enable():
     assert cdist.sum_host(a) is a
     assert cdist.sum_count(7) == 7
     assert not cdist.active()
+
+
+# ----------------------------------------------------------------------------
+# The same through crest_b200.pp / crest_b200.tl themselves: each rank builds
+# a triplet-store BioFrame over its half of the cells (triplet stores take the
+# per-chunk native path), with the oracle standing in for the native module,
+# so the sums at the call sites of pp (QC gene sums, gene statistics, cell
+# count) and tl (scale parameters, Gram / colsum, cell count) are the ones
+# exercised.  Not run on GPUs here: one GPU per call on this build's machines.
+class _OracleNative:
+    """The oracle behind the names pp / tl call on crest_b200._native."""
+
+    qc = staticmethod(oracle.qc)
+    gene_stats = staticmethod(oracle.gene_stats)
+    project = staticmethod(oracle.project)
+    pca_from_gram = staticmethod(oracle.pca_from_gram)
+
+    @staticmethod
+    def gram_accumulate(*args, precision="fp64"):
+        assert precision == "fp64"
+        return oracle.gram_accumulate(*args)
+
+
+def pp_tl_path(indptr, indices, values, lo, hi):
+    import pandas as pd
+    import crest_b200 as cb
+    n = hi - lo
+    cells = np.repeat(np.arange(n, dtype=np.uint32), np.diff(indptr[lo:hi + 1]))
+    g = indices[indptr[lo]:indptr[hi]]
+    v = values[indptr[lo]:indptr[hi]]
+    names = [f"MT-{i}" if i < 5 else f"G{i}" for i in range(N_GENES)]
+    bf = cb.BioFrame.from_triplets(cells, g, v, n, N_GENES, var=pd.DataFrame({"gene_name": names}))
+    bf.chunk_nnz = 5000
+    bf = cb.pp.filter_cells(bf, min_genes=20)
+    bf = cb.pp.filter_genes(bf, min_cells=3)
+    cb.pp.normalize_total(bf, 1e4)
+    cb.pp.log1p(bf)
+    cb.pp.highly_variable_genes(bf, n_top_genes=N_TOP)
+    cb.pp.scale(bf, max_value=10)
+    cb.tl.pca(bf, n_comps=K, gram_precision="fp64")
+    return dict(cells=bf.obs["cell_id"].to_numpy() + lo, genes=bf.var["gene_id"].to_numpy(),
+                hv=bf.var["highly_variable"].to_numpy(), disp=bf.var["dispersions_norm"].to_numpy(),
+                mean_log=bf.var["mean_log"].to_numpy(), X=bf.obsm["X_pca"], variance=bf.uns["pca"]["variance"],
+                loadings=bf.uns["pca"]["projection"]["loadings"])
+
+
+def _rank_pp(rank, world, port, out_dir):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from crest_b200 import dist as cdist, pp, tl
+        pp._native = tl._native = _OracleNative
+        cdist.enable()
+        indptr, indices, values = data()
+        lo, hi = rank * N_CELLS // world, (rank + 1) * N_CELLS // world
+        np.savez(os.path.join(out_dir, f"pp{rank}.npz"), **pp_tl_path(indptr, indices, values, lo, hi))
+        cdist.disable()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_through_pp_and_tl(tmp_path, monkeypatch):
+    world = 2
+    mp.start_processes(_rank_pp, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    from crest_b200 import pp, tl
+    monkeypatch.setattr(pp, "_native", _OracleNative)
+    monkeypatch.setattr(tl, "_native", _OracleNative)
+    indptr, indices, values = data()
+    ref = pp_tl_path(indptr, indices, values, 0, N_CELLS)
+    got = [dict(np.load(tmp_path / f"pp{r}.npz")) for r in range(world)]
+    assert np.array_equal(np.concatenate([x["cells"] for x in got]), ref["cells"])
+    for x in got:
+        assert np.array_equal(x["genes"], ref["genes"])
+        assert np.array_equal(x["hv"], ref["hv"])
+        ok = ~np.isnan(ref["disp"])
+        np.testing.assert_allclose(x["disp"][ok], ref["disp"][ok], rtol=1e-9, atol=1e-12)
+        np.testing.assert_allclose(x["mean_log"], ref["mean_log"], rtol=1e-12)
+        np.testing.assert_allclose(x["variance"], ref["variance"], rtol=1e-10)
+        cos = np.abs((x["loadings"] * ref["loadings"]).sum(0))
+        assert np.all(cos > 1 - 1e-8)
+    # the ranks' scores stacked are the one-process scores (up to sign per component)
+    X = np.concatenate([x["X"] for x in got]).astype(np.float64)
+    R = ref["X"].astype(np.float64)
+    s = np.sign((X * R).sum(0))
+    np.testing.assert_allclose(X * s, R, rtol=1e-4, atol=1e-4 * np.abs(R).max())

@@ -53,3 +53,26 @@ def test_oracle_pipeline_matches_reference_golden(name):
     assert np.array_equal(f.uns["pca"]["variance_ratio"], g["variance_ratio"])
     X = f.obsm["X_pca"][: len(g["X_pca"])]
     assert np.array_equal(X, g["X_pca"])
+
+
+@pytest.mark.parametrize("name", ["small", "pbmc3k_like"])
+def test_oracle_rank_genes_groups_matches_reference_golden(name):
+    """rank_genes_groups (t-test, each synthetic cluster vs the rest) of the
+    reference's crest/tl.py, run on the oracle's native functions, against the
+    oracle's restatement of that host arithmetic: identical tables."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    c, (indptr, indices, data, n_genes, names), g = load_case(name)
+    labels = mg.case_labels(name)
+    f = op.Frame(indptr, indices, data, n_genes, names, threads=THREADS)
+    f = op.filter_cells(f, min_genes=c["min_genes"])
+    f = op.filter_genes(f, min_cells=c["min_cells"])
+    op.normalize_total(f, 1e4)
+    op.log1p(f)
+    tab = op.rank_genes_groups(f, [f"c{x}" for x in labels[f.cell_ids]], n_genes=mg.DE_TOP)
+    assert np.array_equal(tab["group"], g["de_group"])
+    assert np.array_equal(tab["names"], g["de_names"])
+    for k in ("scores", "logfoldchanges", "pvals", "pvals_adj"):
+        assert np.array_equal(tab[k], g[f"de_{k}"]), k
