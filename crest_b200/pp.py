@@ -175,7 +175,8 @@ def group_gene_sums(bf: BioFrame, group_of_row: np.ndarray, n_groups: int, clip:
                 _native.group_gene_sums(*ctx, grp, s, q, z, c)
             else:
                 _native.group_gene_totals(*ctx, grp, s)
-    return (s, q, z) if stats else s
+    # sums over the cells of every rank (identity in one process)
+    return (dist.sum_host(s), dist.sum_host(q), dist.sum_host(z)) if stats else dist.sum_host(s)
 
 
 def _mean_var(s1: np.ndarray, s2: np.ndarray, n: int):
@@ -199,13 +200,27 @@ def _cut_codes(x: np.ndarray, n_bins: int) -> np.ndarray:
 def highly_variable_genes(bf: BioFrame, n_top_genes: Optional[int] = None, flavor: str = "seurat",
                           n_bins: int = 20, min_mean: float = 0.0125, max_mean: float = 3.0,
                           min_disp: float = 0.5, max_disp: float = np.inf, subset: bool = False,
-                          batch_key: Optional[str] = None) -> BioFrame:
-    """``sc.pp.highly_variable_genes`` for ``flavor="seurat"`` (log-normalised data) and
-    ``"cell_ranger"`` (crest/pp.py:201-292).  Adds var columns ``means``, ``dispersions``,
-    ``dispersions_norm``, ``highly_variable``, ``mean_log``, ``std_log``, ``n_cells_expr``
-    and records the ops the log-scale mean/std were computed under (for ``tl.pca``)."""
+                          batch_key: Optional[str] = None, span: float = 0.3) -> BioFrame:
+    """``sc.pp.highly_variable_genes`` for ``flavor="seurat"`` (log-normalised data),
+    ``"cell_ranger"`` and ``"seurat_v3"`` / ``"seurat_v3_paper"`` (crest/pp.py:139-292).
+
+    seurat / cell_ranger add var columns ``means``, ``dispersions``,
+    ``dispersions_norm``, ``highly_variable``, ``mean_log``, ``std_log``,
+    ``n_cells_expr`` and record the ops the log-scale mean/std were computed under
+    (for ``tl.pca``).  seurat_v3 works on the raw counts whatever ops are recorded
+    (``n_top_genes`` required, ``batch_key`` optional) and adds ``means``,
+    ``variances``, ``variances_norm``, ``highly_variable_rank``,
+    ``highly_variable_nbatches``, ``highly_variable``."""
     if flavor in ("seurat_v3", "seurat_v3_paper"):
-        raise NotImplementedError("flavor='seurat_v3' is outside this package's hot path")
+        if n_top_genes is None:
+            raise ValueError("flavor='seurat_v3' needs n_top_genes")
+        cols = _hvg_seurat_v3(bf, int(n_top_genes), batch_key, span, flavor)
+        for name, v in cols.items():
+            bf.var[name] = v
+        bf.uns["hvg"] = {"flavor": flavor}
+        if subset:
+            return bf._subset(var_mask=cols["highly_variable"])
+        return bf
     if batch_key is not None:
         raise NotImplementedError("batch_key is supported for flavor='seurat_v3' only")
     cols = hvg_from_stats(gene_stats(bf), dist.sum_count(bf.n_obs), n_top_genes, flavor, n_bins, min_mean,
@@ -216,6 +231,59 @@ def highly_variable_genes(bf: BioFrame, n_top_genes: Optional[int] = None, flavo
     if subset:
         return bf._subset(var_mask=cols["highly_variable"])
     return bf
+
+
+def _hvg_seurat_v3(bf: BioFrame, n_top: int, batch_key: Optional[str], span: float, flavor: str) -> dict:
+    """Variance-stabilised HVG ranking of the raw counts (seurat_v3): per batch, a
+    loess trend of log10 variance on log10 mean gives each gene an expected
+    standard deviation; values are clipped at mean + sd * sqrt(cells) and the
+    clipped standardised variance ranks the genes.  Two GPU passes of per
+    (batch, gene) sums; the rest is host arithmetic over genes."""
+    from .loess import loess_fit
+    V = bf.n_vars
+    if batch_key is None:
+        grp = np.zeros(bf.n_obs, np.uint32)
+        n_b = 1
+    else:
+        labels = bf.obs[batch_key].astype(str).to_numpy()
+        cats = np.unique(labels)
+        grp = np.searchsorted(cats, labels).astype(np.uint32)
+        n_b = len(cats)
+    cells = dist.sum_host(np.bincount(grp, minlength=n_b).astype(np.float64))
+    s, q, _ = group_gene_sums(bf, grp, n_b, transform=False)
+    mean_all, var_all = _mean_var(s.sum(0), q.sum(0), dist.sum_count(bf.n_obs))
+    cap = np.zeros((n_b, V))
+    mean_b, sd_b = np.zeros((n_b, V)), np.zeros((n_b, V))
+    for b in range(n_b):
+        mean, var = _mean_var(s[b], q[b], int(cells[b]))
+        varying = var > 0
+        trend = np.zeros(V)
+        trend[varying] = loess_fit(np.log10(mean[varying]), np.log10(var[varying]), span=span, degree=2)
+        sd_b[b] = np.sqrt(10 ** trend)
+        mean_b[b] = mean
+        cap[b] = sd_b[b] * np.sqrt(cells[b]) + mean
+    cs, cq, _ = group_gene_sums(bf, grp, n_b, clip=np.ascontiguousarray(cap), transform=False)
+    norm = (1.0 / ((cells[:, None] - 1) * sd_b ** 2)) * (cells[:, None] * mean_b ** 2 + cq - 2 * cs * mean_b)
+    # the per-batch rank of every gene, with numpy's default (unstable) sort as
+    # scanpy uses, so exactly tied genes rank as there
+    rank = np.argsort(np.argsort(-norm, axis=1), axis=1).astype(np.float32)
+    in_top = (rank < n_top).sum(0)
+    rank[rank >= n_top] = np.nan
+    with np.errstate(all="ignore"):
+        import warnings
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore", RuntimeWarning)
+            median_rank = np.nanmedian(rank, axis=0)
+    unranked_last = np.where(np.isnan(median_rank), np.inf, median_rank)
+    if flavor == "seurat_v3":  # median rank, then number of batches; stable
+        order = np.lexsort((-in_top, unranked_last))
+    else:  # seurat_v3_paper: number of batches first
+        order = np.lexsort((unranked_last, -in_top))
+    hv = np.zeros(V, bool)
+    hv[order[:n_top]] = True
+    return {"means": mean_all, "variances": var_all, "variances_norm": norm.mean(0),
+            "highly_variable_rank": median_rank, "highly_variable_nbatches": in_top.astype(np.int64),
+            "highly_variable": hv}
 
 
 def hvg_from_stats(st: np.ndarray, n: int, n_top_genes: Optional[int] = None, flavor: str = "seurat",

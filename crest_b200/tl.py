@@ -226,7 +226,7 @@ def rank_genes_groups(bf: BioFrame, groupby: str, method: str = "t-test", groups
     none = np.iinfo(np.uint32).max
     grp = np.array([index.get(x, none) if x is not None else none for x in labels], dtype=np.uint32)
     G = len(cats)
-    sizes = np.bincount(grp[grp != none], minlength=G).astype(np.float64)
+    sizes = dist.sum_host(np.bincount(grp[grp != none], minlength=G).astype(np.float64))
     N = sizes.sum()
     s, q, _ = group_gene_sums(bf, grp, G)
     s_all, q_all = s.sum(0), q.sum(0)

@@ -31,6 +31,7 @@ REF = None  # the reference checkout, from the command line
 OUT = os.path.dirname(os.path.abspath(__file__))
 THREADS = 4  # rayon thread count emulated by the oracle (fixes the per-gene sum order)
 DE_TOP = 25  # genes per group kept in the differential-expression fixture
+V3_TOP = 200  # seurat_v3 HVG count of the fixture
 
 
 # ------------------------------------------------------------------ fake polars
@@ -86,11 +87,24 @@ class DataFrame:
     def __getitem__(self, k):
         return Series(k, self.cols[k])
 
-    def with_columns(self, series):
+    def with_columns(self, *series):
         d = DataFrame()
         d.cols = dict(self.cols)
-        for s in (series if isinstance(series, (list, tuple)) else [series]):
+        items = series[0] if len(series) == 1 and isinstance(series[0], (list, tuple)) else series
+        for s in items:
             d.cols[s.name] = np.asarray(s.v)
+        return d
+
+    def sort(self, by, descending, nulls_last=True, maintain_order=True):
+        """Stable multi-key sort; NaN / None sort after every number (polars' order)."""
+        keys = []
+        for name, desc in zip(by, descending):
+            v = self.cols[name].astype(float)
+            v = np.where(np.isnan(v), np.inf, -v if desc else v) if not desc else np.where(np.isnan(v), np.inf, -v)
+            keys.append(v)
+        order = np.lexsort(tuple(reversed(keys)))
+        d = DataFrame()
+        d.cols = {k: v[order] for k, v in self.cols.items()}
         return d
 
     def filter(self, mask):
@@ -100,8 +114,9 @@ class DataFrame:
         return d
 
     def drop(self, names):
+        names = {names} if isinstance(names, str) else set(names)
         d = DataFrame()
-        d.cols = {k: v for k, v in self.cols.items() if k not in set(names)}
+        d.cols = {k: v for k, v in self.cols.items() if k not in names}
         return d
 
     def hstack(self, other):
@@ -152,12 +167,24 @@ def run_reference(crest, indptr, indices, data, n_genes, names, n_top, n_comps, 
     crest.pp.scale(bf, max_value=10)
     crest.tl.pca(bf, n_comps=n_comps)
     de = {}
+    if labels is not None:  # seurat_v3 HVG on the raw counts of the filtered cells, with and without batches
+        raw = crest.BioFrame.from_csr(indptr, indices, data, n_genes, var=DataFrame({"gene_name": np.array(names)}))
+        raw = crest.pp.filter_cells(raw, min_genes=min_genes)
+        raw = crest.pp.filter_genes(raw, min_cells=min_cells)
+        kept = raw.obs["cell_id"].to_numpy().astype(np.int64)
+        raw.obs = raw.obs.with_columns(Series("batch", np.array([f"b{x % 3}" for x in labels[kept]])))
+        for tag, key in (("v3", None), ("v3b", "batch")):
+            crest.pp.highly_variable_genes(raw, flavor="seurat_v3", n_top_genes=V3_TOP, batch_key=key)
+            for col in ("means", "variances", "variances_norm", "highly_variable_rank",
+                        "highly_variable_nbatches", "highly_variable"):
+                v = raw.var[col].to_numpy()
+                de[f"{tag}_{col}"] = v.astype(float) if v.dtype == object else v
     if labels is not None:  # differential expression of the synthetic clusters (t-test, each vs rest)
         kept = bf.obs["cell_id"].to_numpy().astype(np.int64)
         bf.obs = bf.obs.with_columns(Series("cluster", np.array([f"c{x}" for x in labels[kept]])))
         tab = crest.tl.rank_genes_groups(bf, "cluster", method="t-test", n_genes=DE_TOP)
-        de = {f"de_{k}": tab[k].to_numpy() for k in ("group", "names", "scores", "logfoldchanges", "pvals",
-                                                      "pvals_adj")}
+        de.update({f"de_{k}": tab[k].to_numpy() for k in ("group", "names", "scores", "logfoldchanges", "pvals",
+                                                           "pvals_adj")})
         de["de_group"] = de["de_group"].astype(str)
         de["de_names"] = de["de_names"].astype(str)
     return {**de,
@@ -217,8 +244,29 @@ def case_input(name):
     return indptr, indices, data, n_genes, synth.gene_names(n_genes)
 
 
+def loess_fixture(crest):
+    """Fits of the reference's loess (crest/_loess.py) on seeded (x, y) sets:
+    mean-variance clouds like seurat_v3's, a smooth curve, and data with ties."""
+    from crest._loess import loess_fit
+    rng = np.random.default_rng(5)
+    out = {}
+    x1 = rng.normal(-1.0, 1.0, 800)
+    y1 = 1.2 * x1 + 0.3 * x1 ** 2 + rng.normal(0, 0.2, 800)
+    x2 = np.linspace(0, 6, 300)
+    y2 = np.sin(x2) + rng.normal(0, 0.05, 300)
+    x3 = np.round(rng.uniform(0, 3, 500), 1)  # many exact ties
+    y3 = np.exp(-x3) + rng.normal(0, 0.02, 500)
+    for i, (x, y, span) in enumerate(((x1, y1, 0.3), (x2, y2, 0.5), (x3, y3, 0.3))):
+        out[f"x{i}"], out[f"y{i}"], out[f"span{i}"] = x, y, np.array([span])
+        out[f"fit{i}"] = loess_fit(x, y, span=span, degree=2)
+    path = os.path.join(OUT, "loess.npz")
+    np.savez_compressed(path, **out)
+    print(path, os.path.getsize(path), "bytes")
+
+
 def main():
     crest = install_fakes()
+    loess_fixture(crest)
     for name, c in CASES.items():
         indptr, indices, data, n_genes, names = case_input(name)
         res = run_reference(crest, indptr, indices, data, n_genes, names, c["n_top"], c["n_comps"], c["min_genes"],

@@ -106,3 +106,38 @@ def test_rank_genes_groups_matches_reference_golden(name, store):
     np.testing.assert_allclose(tab["pvals"].to_numpy(), g["de_pvals"], rtol=1e-6, atol=1e-300)
     np.testing.assert_allclose(tab["pvals_adj"].to_numpy(), g["de_pvals_adj"], rtol=1e-6, atol=1e-300)
     assert "rank_genes_groups" in bf.uns
+
+
+@pytest.mark.parametrize("name", ["small", "pbmc3k_like"])
+@pytest.mark.parametrize("store", ["csr", "triplets"])
+def test_seurat_v3_matches_reference_golden(name, store):
+    """seurat_v3 HVG (two GPU passes of per (batch, gene) sums of the raw
+    counts, the second clipped; loess trend and ranking on the host) against
+    the reference's columns: the HVG set, ranks and batch counts identical,
+    means / variances within 1e-12 relative, variances_norm within 1e-9."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(HERE, "golden", "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    c = mg.CASES[name]
+    indptr, indices, data, n_genes, names = mg.case_input(name)
+    labels = mg.case_labels(name)
+    g = dict(np.load(os.path.join(HERE, "golden", f"{name}.npz")))
+    var = pd.DataFrame({"gene_name": names})
+    if store == "csr":
+        bf = cb.BioFrame.from_csr(indptr, indices, data, n_genes, var=var)
+    else:
+        cells = np.repeat(np.arange(len(indptr) - 1), np.diff(indptr)).astype(np.uint32)
+        bf = cb.BioFrame.from_triplets(cells, indices, data, len(indptr) - 1, n_genes, var=var)
+    bf = cb.pp.filter_cells(bf, min_genes=c["min_genes"])
+    bf = cb.pp.filter_genes(bf, min_cells=c["min_cells"])
+    bf.obs["batch"] = [f"b{x % 3}" for x in labels[bf.obs["cell_id"].to_numpy()]]
+    for tag, key in (("v3", None), ("v3b", "batch")):
+        cb.pp.highly_variable_genes(bf, flavor="seurat_v3", n_top_genes=mg.V3_TOP, batch_key=key)
+        assert np.array_equal(bf.var["highly_variable"].to_numpy(), g[f"{tag}_highly_variable"])
+        assert np.array_equal(bf.var["highly_variable_nbatches"].to_numpy(), g[f"{tag}_highly_variable_nbatches"])
+        assert np.array_equal(bf.var["highly_variable_rank"].to_numpy(), g[f"{tag}_highly_variable_rank"],
+                              equal_nan=True)
+        for col in ("means", "variances"):
+            np.testing.assert_allclose(bf.var[col].to_numpy(), g[f"{tag}_{col}"], rtol=1e-12)
+        np.testing.assert_allclose(bf.var["variances_norm"].to_numpy(), g[f"{tag}_variances_norm"], rtol=1e-9)
