@@ -7,7 +7,8 @@ tensor cores), FP64 centring and eigensolve, and the score projection.
 
 __version__ = "0.1.0"
 
-from .core import BioFrame, CSRStore, FrameStore, DeviceMatrix  # noqa: F401
+from .core import BioFrame, CSRStore, FrameStore, ParquetStore, DeviceMatrix, read_parquet  # noqa: F401
 from . import pp, tl  # noqa: F401
 
-__all__ = ["BioFrame", "CSRStore", "FrameStore", "DeviceMatrix", "pp", "tl", "__version__"]
+__all__ = ["BioFrame", "CSRStore", "FrameStore", "ParquetStore", "DeviceMatrix", "read_parquet", "pp", "tl",
+           "__version__"]

@@ -13,6 +13,8 @@ Stores:
   (:meth:`CSRStore.device_matrix`) or stream pinned host chunks.
 * :class:`FrameStore` - COO ``(cell_id, gene_id, count)`` triplets sorted by
   cell, processed chunk by chunk through the per-chunk native functions.
+* :class:`ParquetStore` - the same triplets on disk as Parquet parts, read one
+  part at a time (out of core) with the next part decoded in the background.
 """
 
 from __future__ import annotations
@@ -132,7 +134,48 @@ class FrameStore:
             lo = hi
 
 
-Store = Union[CSRStore, FrameStore]
+class ParquetStore:
+    """Raw counts on disk, out of core: a directory of ``part-*.parquet`` files of
+    ``(cell_id, gene_id, count)`` rows, each file holding whole cells in cell
+    order (crest/core.py:108-135).  One chunk is one file; while the GPU works
+    on a chunk, a reader thread already decodes the next file, so disk and
+    decompression overlap the device passes.  Made by
+    :meth:`BioFrame.write_parquet`, opened with :func:`read_parquet`."""
+
+    def __init__(self, path, n_cells: int, n_genes: int):
+        from pathlib import Path
+        self.path = Path(path)
+        self.parts = sorted(self.path.glob("part-*.parquet"))
+        if not self.parts:
+            raise FileNotFoundError(f"no part-*.parquet files in {self.path}")
+        self.n_cells, self.n_genes = int(n_cells), int(n_genes)
+
+    @property
+    def nnz(self) -> int:
+        import pyarrow.parquet as pq
+        return int(sum(pq.ParquetFile(p).metadata.num_rows for p in self.parts))
+
+    @staticmethod
+    def _read(part):
+        import pyarrow.parquet as pq
+        t = pq.read_table(part, columns=["cell_id", "gene_id", "count"])
+        col = {name: t.column(name).to_numpy() for name in ("cell_id", "gene_id", "count")}
+        return (np.ascontiguousarray(col["gene_id"], dtype=np.uint32),
+                np.ascontiguousarray(col["count"], dtype=np.float32),
+                np.ascontiguousarray(col["cell_id"], dtype=np.uint32))
+
+    def chunks(self, chunk_nnz: int = DEFAULT_CHUNK_NNZ):
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(max_workers=1) as pool:
+            nxt = pool.submit(self._read, self.parts[0])
+            for i in range(len(self.parts)):
+                genes, values, cells = nxt.result()
+                if i + 1 < len(self.parts):
+                    nxt = pool.submit(self._read, self.parts[i + 1])
+                yield genes, values, cells, None, 0
+
+
+Store = Union[CSRStore, FrameStore, ParquetStore]
 
 
 @dataclass
@@ -278,6 +321,78 @@ class BioFrame:
         """Keep genes where the boolean mask holds."""
         return self._subset(var_mask=np.asarray(mask, dtype=bool))
 
+    def raw_triplets(self) -> Iterator[tuple]:
+        """Raw counts of the kept cells / genes with their current row / column ids,
+        chunk by chunk: ``(rows u32, cols u32, counts f32)``, cell-sorted."""
+        cmap, gmap = self._cell_map(), self._gene_map()
+        for genes, values, cells, indptr, first in self.store.chunks(self.chunk_nnz):
+            if cells is None:
+                cells = first + np.repeat(np.arange(len(indptr) - 1, dtype=np.int64), np.diff(indptr))
+            cells = np.asarray(cells, dtype=np.int64)
+            ok = cells < len(cmap)
+            rows = np.full(len(cells), -1, np.int64)
+            rows[ok] = cmap[cells[ok]]
+            g = np.asarray(genes, dtype=np.int64)
+            okg = g < len(gmap)
+            cols = np.full(len(g), -1, np.int64)
+            cols[okg] = gmap[g[okg]]
+            keep = (rows >= 0) & (cols >= 0)
+            yield rows[keep].astype(np.uint32), cols[keep].astype(np.uint32), np.asarray(values, np.float32)[keep]
+
+    def write_parquet(self, path, nnz_per_part: int = 1 << 23) -> None:
+        """Write the raw counts of the kept cells / genes (current ids) as a Parquet
+        directory of whole-cell parts of about ``nnz_per_part`` stored values, with
+        ``obs.parquet`` / ``var.parquet`` (crest/core.py:368-392)."""
+        from pathlib import Path
+        import pyarrow as pa
+        import pyarrow.parquet as pq
+        path = Path(path)
+        path.mkdir(parents=True, exist_ok=True)
+        for old in path.glob("part-*.parquet"):
+            old.unlink()
+        pending, n_pending, part = [], 0, 0
+
+        def flush():
+            nonlocal pending, n_pending, part
+            if pending:
+                cols = [np.concatenate([p[i] for p in pending]) for i in range(3)]
+                table = pa.table({"cell_id": cols[0], "gene_id": cols[1], "count": cols[2]})
+                pq.write_table(table, path / f"part-{part:05d}.parquet", compression="zstd")
+                part += 1
+            pending, n_pending = [], 0
+
+        for r, g, v in self.raw_triplets():
+            lo = 0
+            while lo < len(r):
+                hi = min(lo + nnz_per_part - n_pending, len(r))
+                if hi < len(r):  # a part ends where a cell ends
+                    hi = int(np.searchsorted(r, r[hi - 1], side="right"))
+                pending.append((r[lo:hi], g[lo:hi], v[lo:hi]))
+                n_pending += hi - lo
+                lo = hi
+                if n_pending >= nnz_per_part:
+                    flush()
+        flush()
+        obs = self.obs.copy()
+        obs["cell_id"] = np.arange(self.n_obs, dtype=np.uint32)
+        var = self.var.copy()
+        var["gene_id"] = np.arange(self.n_vars, dtype=np.uint32)
+        pq.write_table(pa.Table.from_pandas(obs, preserve_index=False), path / "obs.parquet")
+        pq.write_table(pa.Table.from_pandas(var, preserve_index=False), path / "var.parquet")
+
     def copy(self) -> "BioFrame":
         return BioFrame(self.store, self.obs.copy(), self.var.copy(), dict(self.obsm), dict(self.varm),
                         dict(self.uns), list(self.ops), self.chunk_nnz)
+
+
+def read_parquet(path, chunk_nnz: int = DEFAULT_CHUNK_NNZ) -> BioFrame:
+    """Open a Parquet directory written by :meth:`BioFrame.write_parquet` (out of
+    core: passes read one part at a time; crest/core.py:414-421)."""
+    from pathlib import Path
+    import pyarrow.parquet as pq
+    path = Path(path)
+    obs = pq.read_table(path / "obs.parquet").to_pandas()
+    var = pq.read_table(path / "var.parquet").to_pandas()
+    bf = BioFrame._with_store(ParquetStore(path, len(obs), len(var)), obs, var)
+    bf.chunk_nnz = chunk_nnz
+    return bf

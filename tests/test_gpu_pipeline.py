@@ -147,3 +147,16 @@ def test_precision_forms_against_fp64():
         sep = separated(ref.uns["pca"]["variance"])
         assert aligned_rel_err(got.obsm["X_pca"], ref.obsm["X_pca"], sep) <= 1e-4
         assert procrustes_rel_err(got.obsm["X_pca"], ref.obsm["X_pca"]) <= 1e-4
+
+
+def test_parquet_store_matches_csr_store(tmp_path):
+    """The out-of-core Parquet store (parts read one at a time, per-chunk GPU
+    passes) gives the CSR store's result (crest's own test_stores_agree)."""
+    c, inp, g = load_case("small")
+    a = pipeline(frame(inp), c, "fp64")
+    bf = frame(inp)
+    bf.write_parquet(tmp_path, nnz_per_part=40_000)
+    p = pipeline(cb.read_parquet(tmp_path), c, "fp64")
+    assert np.array_equal(p.var["highly_variable"].to_numpy(), a.var["highly_variable"].to_numpy())
+    assert max_angle(p.obsm["X_pca"], a.obsm["X_pca"]) <= 1e-4
+    assert aligned_rel_err(p.obsm["X_pca"], a.obsm["X_pca"]) <= 1e-5
