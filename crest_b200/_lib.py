@@ -63,6 +63,7 @@ _SIGS = {
     "crest_gene_stats": [P, I64, P],
     "crest_group_gene_sums": [P, P, I64, I64, I64, P, P, P, P],
     "crest_group_gene_totals": [P, P, I64, I64, I64, P],
+    "crest_knn_graph": [P, I64, I64, I64, P, P],
     "crest_gram_accumulate": [P, P, I64, P, I64, P, P, I32],
     "crest_pca_from_gram": [P, P, I64, I64, I64, P, P, P, P],
     "crest_project": [P, P, I64, P, I64, I64, P, P, I64],

@@ -20,7 +20,7 @@ from . import _lib
 from ._lib import carray, ptr
 
 __all__ = ["qc", "gene_stats", "gram_accumulate", "pca_from_gram", "project", "group_gene_sums",
-           "group_gene_totals", "t_pvalues"]
+           "group_gene_totals", "t_pvalues", "knn_graph"]
 
 
 def _chunk(genes, values, cell_map, gene_map, target_sum, log1p, cells, indptr, first_cell):
@@ -207,3 +207,22 @@ def t_pvalues(t, df):
     p = np.full(t.shape, np.nan)
     p[ok] = np.minimum(2.0 * stdtr(df[ok], -np.abs(t[ok])), 1.0)
     return p
+
+
+def knn_graph(data, k, exact=None, seed=0):
+    """k nearest neighbours of every row of ``data`` (n x d f32), self excluded, ascending
+    distance (src/py.rs:52-72).  Returns (indices u32 (n, k'), distances f32 (n, k')) with
+    k' = min(k, n - 1).  The search is always exhaustive (``exact`` and ``seed`` are
+    accepted for the reference's signature; there is no approximate index)."""
+    X = np.asarray(data)
+    if X.ndim != 2 or X.dtype != np.float32:
+        raise TypeError("data must be a 2-d float32 array")
+    if not X.flags.c_contiguous:
+        raise ValueError("data must be C-contiguous")
+    n, d = X.shape
+    kk = max(1, min(int(k), n - 1)) if n > 1 else 0
+    idx = np.zeros((n, kk), np.uint32)
+    dist = np.zeros((n, kk), np.float32)
+    if kk:
+        _lib.call("crest_knn_graph", ptr(X), n, d, int(k), ptr(idx), ptr(dist))
+    return idx, dist

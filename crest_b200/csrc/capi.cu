@@ -544,6 +544,25 @@ int crest_group_gene_totals(const crest_chunk *chunk, const uint32_t *group_of_r
                                  nullptr);
 }
 
+int crest_knn_graph(const float *data, int64_t n, int64_t d, int64_t k, uint32_t *indices, float *distances) {
+    CREST_REQUIRE(n >= 0 && d >= 1 && k >= 0 && (n == 0 || data), CREST_EINVAL, "data must be (n, d) with d >= 1");
+    const int64_t kk = n > 1 ? std::max<int64_t>(1, std::min(k, n - 1)) : 0;
+    if (kk == 0) return CREST_OK;
+    CREST_REQUIRE(indices && distances, CREST_EINVAL, "NULL output");
+    Ctx *x;
+    CREST_TRY(get_ctx(&x));
+    std::lock_guard<std::mutex> lock(x->mu);
+    cudaStream_t st = x->st;
+    CREST_TRY(upload(x->out0, data, n * d, st));
+    CREST_TRY(x->out1.ensure(sizeof(uint32_t) * (size_t)(n * kk)));
+    CREST_TRY(x->out2.ensure(sizeof(float) * (size_t)(n * kk)));
+    CREST_TRY(launch_knn(x->out0.as<float>(), n, (int)d, (int)kk, x->out1.as<uint32_t>(), x->out2.as<float>(), st));
+    CREST_CUDA_TRY(cudaMemcpyAsync(indices, x->out1.ptr, 4 * (size_t)(n * kk), cudaMemcpyDeviceToHost, st));
+    CREST_CUDA_TRY(cudaMemcpyAsync(distances, x->out2.ptr, 4 * (size_t)(n * kk), cudaMemcpyDeviceToHost, st));
+    CREST_CUDA_TRY(cudaStreamSynchronize(st));
+    return CREST_OK;
+}
+
 int crest_project(const crest_chunk *chunk, const int32_t *sub_map, int64_t n_vars, const double *loadings,
                   int64_t d, int64_t k, const crest_scale *scale, float *out, int64_t n_rows) {
     CREST_TRY(validate_chunk(chunk));

@@ -25,6 +25,8 @@ struct RowOut {  // per-row QC results added at the cell's row (matrix API)
 int launch_qc(const DevChunk &c, const uint8_t *flag, uint32_t *gene_ncells, double *gene_total,
               const SpanOut *span, const RowOut *row, cudaStream_t st);
 int launch_gene_stats(const DevChunk &c, double *out, cudaStream_t st);
+// Exact k nearest neighbours (self excluded) of the rows of X (n x d f32, device).
+int launch_knn(const float *X, int64_t n, int d, int k, uint32_t *idx, float *dist, cudaStream_t st);
 // Per (group, var) sums of the transformed values (sumsq / nnz / clip may be NULL).
 int launch_group_gene_sums(const DevChunk &c, const uint32_t *group_of_row, int64_t n_vars, const double *clip,
                            double *sum, double *sumsq, double *nnz, cudaStream_t st);

@@ -21,7 +21,8 @@ from . import _lib, _native, dist
 from .core import BioFrame
 
 __all__ = ["calculate_qc_metrics", "filter_cells", "filter_genes", "normalize_total", "log1p", "scale",
-           "gene_stats", "group_gene_sums", "highly_variable_genes", "hvg_from_stats"]
+           "gene_stats", "group_gene_sums", "highly_variable_genes", "hvg_from_stats", "neighbors",
+           "connectivities", "connectivities_matrix"]
 
 
 # --------------------------------------------------------------------------- QC
@@ -347,3 +348,85 @@ def hvg_from_stats(st: np.ndarray, n: int, n_top_genes: Optional[int] = None, fl
     std_log[std_log == 0] = 1.0
     return {"means": mean, "dispersions": disp, "dispersions_norm": disp_norm, "highly_variable": hv,
             "mean_log": mean_log, "std_log": std_log, "n_cells_expr": st[:, 4].astype(np.int64)}
+
+
+# --------------------------------------------------------------------------- neighbours
+def neighbors(bf: BioFrame, n_neighbors: int = 15, n_pcs: Optional[int] = None, use_rep: str = "X_pca",
+              exact: Optional[bool] = None, random_state: int = 0) -> BioFrame:
+    """kNN graph of the cells on ``obsm[use_rep]`` plus UMAP fuzzy connectivities
+    (``sc.pp.neighbors(method="umap")``; crest/pp.py:296-315).  ``n_neighbors``
+    counts the cell itself, as in scanpy.  The neighbours are exact for every
+    number of cells (exhaustive GPU search); ``exact`` and ``random_state`` are
+    accepted for the reference's signature."""
+    if use_rep not in bf.obsm:
+        raise KeyError(f"{use_rep!r} not in obsm; run crest_b200.tl.pca first")
+    X = bf.obsm[use_rep]
+    if n_pcs is not None:
+        X = X[:, :n_pcs]
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    idx, dist = _native.knn_graph(X, n_neighbors - 1, exact=exact, seed=random_state)
+    rows, cols, w = connectivities(idx, dist, n_neighbors)
+    bf.uns["neighbors"] = {
+        "params": {"n_neighbors": n_neighbors, "n_pcs": n_pcs, "use_rep": use_rep, "method": "umap"},
+        "indices": idx, "distances": dist, "rows": rows, "cols": cols, "weights": w,
+    }
+    return bf
+
+
+def connectivities(indices: np.ndarray, distances: np.ndarray, n_neighbors: int):
+    """UMAP's fuzzy simplicial set of a kNN graph (McInnes, Healy & Melville 2018,
+    with umap-learn's published smoothing constants): per cell, rho = distance to
+    its nearest neighbour and sigma from a 64-step bisection making the memberships
+    exp(-(d - rho) / sigma) of its n_neighbors - 1 neighbours sum to
+    log2(n_neighbors), floored at 1e-3 of the cell's mean distance (self included
+    as 0); the directed memberships are combined by fuzzy union a + b - a b.
+    Returns the undirected edges (rows < cols) with their weights."""
+    idx = np.asarray(indices, np.int64)
+    d = np.asarray(distances, np.float64)
+    n, k = d.shape
+    if n == 0 or k == 0:
+        return np.zeros(0, np.uint32), np.zeros(0, np.uint32), np.zeros(0, np.float32)
+    target = np.log2(n_neighbors)
+    pos = np.where(d > 0, d, np.inf)
+    rho = pos.min(axis=1)
+    rho[~np.isfinite(rho)] = 0.0
+    lo, hi, mid = np.zeros(n), np.full(n, np.inf), np.ones(n)
+    done = np.zeros(n, bool)
+    for _ in range(64):
+        gap = d - rho[:, None]
+        psum = np.where(gap > 0, np.exp(-gap / mid[:, None]), 1.0).sum(axis=1)
+        done |= np.abs(psum - target) < 1e-5
+        act = ~done
+        big = act & (psum > target)
+        hi = np.where(big, mid, hi)
+        small = act & ~big
+        lo = np.where(small, mid, lo)
+        mid = np.where(big, (lo + hi) / 2, np.where(small, np.where(np.isinf(hi), mid * 2, (lo + hi) / 2), mid))
+        if done.all():
+            break
+    mean_all = d.sum() / (n * (k + 1))
+    mean_i = d.sum(axis=1) / (k + 1)
+    sigma = np.where(rho > 0, np.maximum(mid, 1e-3 * mean_i), np.maximum(mid, 1e-3 * mean_all))
+    gap = d - rho[:, None]
+    w = np.where(gap > 0, np.exp(-gap / sigma[:, None]), 1.0)
+    src = np.repeat(np.arange(n), k)
+    dst = idx.ravel()
+    ok = (dst >= 0) & (dst < n) & (dst != src)
+    a, b, wv = np.minimum(src, dst)[ok], np.maximum(src, dst)[ok], w.ravel()[ok]
+    key = a * n + b
+    order = np.argsort(key, kind="stable")
+    key, wv = key[order], wv[order]
+    uniq, first, count = np.unique(key, return_index=True, return_counts=True)
+    w1 = wv[first]
+    w2 = np.where(count > 1, wv[np.minimum(first + 1, len(wv) - 1)], 0.0)
+    weight = w1 + w2 - w1 * w2
+    return (uniq // n).astype(np.uint32), (uniq % n).astype(np.uint32), weight.astype(np.float32)
+
+
+def connectivities_matrix(bf: BioFrame):
+    """Symmetric scipy.sparse CSR connectivities (scanpy ``obsp['connectivities']``)."""
+    import scipy.sparse as sp
+    nb = bf.uns["neighbors"]
+    n = bf.n_obs
+    C = sp.coo_matrix((nb["weights"], (nb["rows"], nb["cols"])), shape=(n, n)).tocsr()
+    return (C + C.T).tocsr()

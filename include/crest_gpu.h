@@ -128,6 +128,13 @@ int crest_group_gene_sums(const crest_chunk *chunk, const uint32_t *group_of_row
 int crest_group_gene_totals(const crest_chunk *chunk, const uint32_t *group_of_row, int64_t n_group_rows,
                             int64_t n_groups, int64_t n_vars, double *sum);
 
+/* knn_graph: src/py.rs:52-72, src/knn.rs:337-371.  k nearest neighbours of
+ * every row of data (n x d f32, row-major, host), self excluded, ascending
+ * Euclidean distance, ties by index; k is reduced to min(k, n - 1) (at least
+ * 1 when n > 1).  indices / distances are (n x k') with k' that value.  The
+ * search is exhaustive for every n (exact neighbours); d <= 128, k' <= 64. */
+int crest_knn_graph(const float *data, int64_t n, int64_t d, int64_t k, uint32_t *indices, float *distances);
+
 /* crest_qc_static: no counterpart in the reference.  Same arguments and
  * results as crest_qc, computed without allocating device memory: the
  * kernel runs on a fixed scratch array compiled into the library (about

@@ -73,6 +73,7 @@ def lib():
         L.oc_materialize.restype = C.c_int64
         L.oc_synth.argtypes = [P, P, P, P, P, C.c_int]
         L.oc_group_gene_sums.argtypes = [P, P, C.c_int64, P, P, P, P]
+        L.oc_knn.argtypes = [P, C.c_int64, C.c_int64, C.c_int64, P, P, C.c_int]
         _lib = L
     return _lib
 
@@ -249,6 +250,19 @@ def t_pvalues(t, df):
     p = np.full(t.shape, np.nan)
     p[ok] = np.minimum(2.0 * stats.t.sf(np.abs(t[ok]), df[ok]), 1.0)
     return p
+
+
+def knn_graph(data, k, exact=None, seed=0, threads=None):
+    """src/py.rs:52-72 / src/knn.rs: exact k nearest neighbours (self excluded),
+    (indices u32 (n, k'), distances f32 (n, k')), k' = min(k, n - 1)."""
+    X = _c(np.asarray(data), np.float32, "data")
+    n, d = X.shape
+    kk = max(1, min(int(k), n - 1)) if n > 1 else 0
+    idx = np.zeros((n, kk), np.uint32)
+    dist = np.zeros((n, kk), np.float32)
+    if kk:
+        lib().oc_knn(_ptr(X), n, d, kk, _ptr(idx), _ptr(dist), threads or DEFAULT_THREADS)
+    return idx, dist
 
 
 def pca_from_gram(gram, colsum, n, k):

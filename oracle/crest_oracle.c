@@ -549,3 +549,68 @@ int oc_group_gene_sums(const oc_chunk *v, const uint32_t *group_of_row, int64_t 
     free(bg); free(bx); free(sp);
     return 0;
 }
+
+/* ------------------------------------------------------------------ knn
+ * src/knn.rs: exact k nearest neighbours (self excluded) of the rows of an
+ * n x d f32 matrix.  Distances follow sq_dist (src/knn.rs:48-66): f32
+ * differences squared into eight partial sums over 8-wide chunks, partials
+ * added in order, remaining coordinates one by one, no contraction (built
+ * with -ffp-contract=off); the k best by (distance, index) after the square
+ * root, as the reference's final re-sort (src/knn.rs:357-366).  Exhaustive
+ * for every n: the exact answer the reference's brute force approximates
+ * through GEMM-tile distances for its candidate selection. */
+static float knn_sq(const float *a, const float *b, int64_t d) {
+    float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int64_t full = d - d % 8;
+    for (int64_t c = 0; c < full; c += 8)
+        for (int l = 0; l < 8; l++) {
+            float t = a[c + l] - b[c + l];
+            acc[l] += t * t;
+        }
+    float s = 0.0f;
+    for (int l = 0; l < 8; l++) s += acc[l];
+    for (int64_t j = full; j < d; j++) {
+        float t = a[j] - b[j];
+        s += t * t;
+    }
+    return s;
+}
+
+typedef struct {
+    const float *x;
+    int64_t n, d, k;
+    uint32_t *idx;
+    float *dist;
+} knn_job;
+
+static void knn_rows(void *c_, int64_t i) {
+    knn_job *c = (knn_job *)c_;
+    const int64_t k = c->k;
+    float *bd = c->dist + i * k;
+    uint32_t *bi = c->idx + i * k;
+    for (int64_t j = 0; j < k; j++) { bd[j] = INFINITY; bi[j] = 0xffffffffu; }
+    for (int64_t j = 0; j < c->n; j++) {
+        if (j == i) continue;
+        float s = knn_sq(c->x + i * c->d, c->x + j * c->d, c->d);
+        if (!(s < bd[k - 1])) continue;
+        int64_t p = k - 1;
+        while (p > 0 && bd[p - 1] > s) { bd[p] = bd[p - 1]; bi[p] = bi[p - 1]; p--; }
+        bd[p] = s;
+        bi[p] = (uint32_t)j;
+    }
+    for (int64_t j = 0; j < k; j++) if (bi[j] != 0xffffffffu) bd[j] = sqrtf(bd[j]);
+    for (int64_t j = 1; j < k; j++) {  /* (distance, index) order */
+        float dj = bd[j];
+        uint32_t ij = bi[j];
+        int64_t p = j;
+        while (p > 0 && (bd[p - 1] > dj || (bd[p - 1] == dj && bi[p - 1] > ij))) { bd[p] = bd[p - 1]; bi[p] = bi[p - 1]; p--; }
+        bd[p] = dj;
+        bi[p] = ij;
+    }
+}
+
+int oc_knn(const float *x, int64_t n, int64_t d, int64_t k, uint32_t *idx, float *dist, int n_threads) {
+    knn_job c = {x, n, d, k, idx, dist};
+    run_pool(n_threads, n, knn_rows, &c);
+    return 0;
+}
