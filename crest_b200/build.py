@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcrest_gpu.so")
-SOURCES = ["capi.cu", "capi_matrix.cu", "capi_static.cu", "k_fused.cu", "k_stream.cu", "k_sweep.cu", "k_gram.cu", "k_gram_tc.cu", "k_compact.cu", "k_groups.cu", "k_knn.cu", "k_eig.cu", "synth.cu", "prof.cu"]
+SOURCES = ["capi.cu", "capi_matrix.cu", "capi_static.cu", "k_fused.cu", "k_stream.cu", "k_sweep.cu", "k_gram.cu", "k_gram_tc.cu", "k_compact.cu", "k_groups.cu", "k_knn.cu", "k_csc.cu", "k_eig.cu", "synth.cu", "prof.cu"]
 HEADERS = ["common.cuh", "kernels.cuh", "rowwarp.cuh", "host.cuh", "log1pf_libm.h", "synth_core.h", "prof.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -6,6 +6,7 @@
 // (residency HOST; the reference's out-of-core model, crest/core.py:54-62 and
 // docs/memory_model.md, with device memory bounded by two chunks plus the
 // accumulators).
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -49,6 +50,10 @@ struct crest_matrix {
     std::vector<int32_t> cmp_gene_map, cmp_sub_map;
     double cmp_target = 0.0;
     int64_t cmp_d = -1;
+    // gene-major copy of a device-resident matrix for per-gene statistics
+    // (built on first use; csc_state -1 once it could not be built)
+    crest::CscMatrix csc;
+    int csc_state = 0;
 };
 
 struct crest_pca {
@@ -205,6 +210,31 @@ int range_index(crest_matrix *m, RangeIndex &ix, bool &ok) {
     return CREST_OK;
 }
 
+// The gene-major copy of a device-resident matrix, built on first use;
+// false when the matrix is streamed, the copy does not fit, or
+// CREST_GENE_MAJOR=0 (then the per-gene passes use the gene-range sweep or
+// the entry-parallel kernels).
+int gene_major(crest_matrix *m, bool &ok) {
+    ok = false;
+    if (m->residency != CREST_MEM_DEVICE || m->n_cells == 0 || m->n_genes == 0 || m->csc_state < 0) return CREST_OK;
+    const char *e = getenv("CREST_GENE_MAJOR");
+    if (e && e[0] == '0') return CREST_OK;
+    if (m->csc_state == 0) {
+        const int rc = build_csc(m->d_indptr.as<int64_t>(), m->d_indices.as<uint32_t>(), m->d_data.as<float>(),
+                                 m->n_cells, m->n_genes, m->nnz, m->csc, m->compute);
+        if (rc == CREST_ENOMEM || rc == CREST_EINVAL) {  // no room / unsupported shape: keep the CSR passes
+            m->csc.release();
+            cudaGetLastError();
+            m->csc_state = -1;
+            return CREST_OK;
+        }
+        CREST_TRY(rc);
+        m->csc_state = 1;
+    }
+    ok = true;
+    return CREST_OK;
+}
+
 // Per-cell kept-gene totals of a device-resident matrix for the staged
 // gene_map (cached until the map changes).
 int cell_totals(crest_matrix *m, const int32_t *gene_map, const DevChunk &proto, const double **out) {
@@ -249,6 +279,7 @@ int compact_pass(crest_matrix *m, const DevChunk &proto, int64_t d, bool &done, 
         m->cmp_scale.ensure(8 * n) || m->cmp_status.ensure(sizeof(int)) ||
         m->cls.ensure(4 * gene_class_words(std::max<int64_t>(m->n_genes, 1)))) {
         compact_release(m);
+    m->csc.release();
         cudaGetLastError();
         m->compact_off = true;
         return CREST_OK;
@@ -488,7 +519,15 @@ int crest_matrix_gene_stats(crest_matrix *m, const int64_t *cell_map, const int3
     RangeIndex ix;
     bool swept = false;
     CREST_TRY(range_index(m, ix, swept));
-    if (swept) {  // gene-range sweep over the whole resident matrix
+    bool by_gene = false;
+    CREST_TRY(gene_major(m, by_gene));
+    if (by_gene) {  // segmented reductions over the gene-major copy
+        const double *total = nullptr;
+        if (target_sum > 0.0) CREST_TRY(cell_totals(m, gene_map, proto, &total));
+        DevChunk c = proto;
+        c.n_spans = m->n_cells;
+        CREST_TRY(launch_gene_stats_csc(c, m->csc, total, m->out[0].as<double>(), st));
+    } else if (swept) {  // gene-range sweep over the whole resident matrix
         const double *total = nullptr;
         if (target_sum > 0.0) CREST_TRY(cell_totals(m, gene_map, proto, &total));
         DevChunk c = proto;

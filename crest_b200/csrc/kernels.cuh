@@ -25,6 +25,23 @@ struct RowOut {  // per-row QC results added at the cell's row (matrix API)
 int launch_qc(const DevChunk &c, const uint8_t *flag, uint32_t *gene_ncells, double *gene_total,
               const SpanOut *span, const RowOut *row, cudaStream_t st);
 int launch_gene_stats(const DevChunk &c, double *out, cudaStream_t st);
+// Gene-major copy of a device-resident CSR matrix (k_csc.cu): column g holds
+// (cell, raw value) of its entries in [col_ptr[g], col_ptr[g + 1]); segments
+// of at most 16384 entries of one gene start at seg_lo[s] (gene seg_gene[s]).
+struct CscMatrix {
+    DevBuf col_ptr, col_cell, col_val, seg_lo, seg_gene;
+    int64_t n_segs = 0, n_genes = 0;
+    void release() {
+        for (auto *b : {&col_ptr, &col_cell, &col_val, &seg_lo, &seg_gene}) b->release();
+        n_segs = n_genes = 0;
+    }
+};
+int build_csc(const int64_t *indptr, const uint32_t *genes, const float *values, int64_t n_cells, int64_t n_genes,
+              int64_t nnz, CscMatrix &out, cudaStream_t st);
+// gene_stats of a whole matrix (c: the matrix as one chunk, for its maps and
+// transform) from its gene-major copy, given the per-cell kept-gene totals.
+int launch_gene_stats_csc(const DevChunk &c, const CscMatrix &m, const double *total, double *out, cudaStream_t st);
+
 // Exact k nearest neighbours (self excluded) of the rows of X (n x d f32, device).
 int launch_knn(const float *X, int64_t n, int d, int k, uint32_t *idx, float *dist, cudaStream_t st);
 // Per (group, var) sums of the transformed values (sumsq / nnz / clip may be NULL).

@@ -110,7 +110,11 @@ def test_qc_sweep_equals_streamed_matrix():
 
 @pytest.mark.parametrize("unsorted_rows", [0, 3])
 @pytest.mark.parametrize("target,log", [(1e4, True), (0.0, True), (1e4, False)])
-def test_gene_stats_sweep_matches_oracle(unsorted_rows, target, log):
+@pytest.mark.parametrize("gene_major", ["1", "0"])
+def test_gene_stats_sweep_matches_oracle(unsorted_rows, target, log, gene_major, monkeypatch):
+    """gene_stats from the gene-major copy (default) and from the gene-range
+    sweep / entry-parallel kernels (CREST_GENE_MAJOR=0)."""
+    monkeypatch.setenv("CREST_GENE_MAJOR", gene_major)
     n = 3000
     indptr, idx, val = make(n, 5, True, unsorted_rows, beyond=1)
     cm, gm, nr, nv = maps(n, 6)
@@ -119,7 +123,9 @@ def test_gene_stats_sweep_matches_oracle(unsorted_rows, target, log):
     np.testing.assert_allclose(o[:, :4], r[:, :4], rtol=1e-12, atol=1e-300)
 
 
-def test_gene_stats_sweep_follows_gene_map_changes():
+@pytest.mark.parametrize("gene_major", ["1", "0"])
+def test_gene_stats_sweep_follows_gene_map_changes(gene_major, monkeypatch):
+    monkeypatch.setenv("CREST_GENE_MAJOR", gene_major)
     n = 2000
     indptr, idx, val = make(n, 7, False)
     cm, gm, nr, nv = maps(n, 8)
