@@ -91,24 +91,6 @@ __device__ __forceinline__ void range_window(const int32_t *o, int r, int n_rang
     b = r == n_ranges - 1 ? nnz : (int64_t)__ldg(o + r);
 }
 
-// The next kept cell of this warp (spans i, i + step, ... below c1) and its
-// window of range r; false when none is left.
-__device__ __forceinline__ bool next_window(const DevChunk &c, const RangeIndex &ix, int r, int64_t &i, int64_t c1,
-                                            int64_t step, Win &w) {
-    for (; i < c1; i += step) {
-        int64_t lo, hi;
-        if (span_row(c, i, lo, hi) < 0) continue;
-        int64_t a, b;
-        range_window(ix.off + (c.first_cell + i) * (ix.n_ranges - 1), r, ix.n_ranges, hi - lo, a, b);
-        w.span = i;
-        w.a = lo + a;
-        w.b = lo + b;
-        i += step;
-        return true;
-    }
-    return false;
-}
-
 // Up to kWinU * 32 entries of a window in registers (lane-strided).
 constexpr int kWinU = 8;
 struct WinBuf {
@@ -128,22 +110,60 @@ __device__ __forceinline__ void win_load(const DevChunk &c, int64_t s, int64_t h
 
 // Every window of range r of this warp's cells [c0 + warp, c1) (step
 // n_warps): cell(w) once per window before its entries, entry(g, x, valid)
-// for every lane of each 32-entry group, done(w) after them.  The first
-// kWinU * 32 entries of the next window are loaded before the current one
-// is processed, so each warp keeps two windows of loads in flight.
+// for every lane of each 32-entry group, done(w) after them.  The windows'
+// bounds are fetched 32 cells at a time (lane j reads the row bounds, the
+// cell map and the range offsets of the j-th next cell of this warp, one
+// round trip for 32 windows instead of three dependent loads per window),
+// and the first kWinU * 32 entries of the next window are loaded before the
+// current one is processed, so each warp keeps two windows of loads in
+// flight.
 template <class C, class E, class D>
 __device__ __forceinline__ void sweep_range(const DevChunk &c, const RangeIndex &ix, int r, int64_t c0, int64_t c1,
                                             C &&cell, E &&entry, D &&done) {
     const int lane = lane_id();
     const int64_t step = blockDim.x >> 5;
-    int64_t i = c0 + (threadIdx.x >> 5);
     constexpr int64_t kSpan = kWinU * 32;
+    int64_t batch = c0 + (threadIdx.x >> 5);  // this warp's first cell of the current batch
+    int64_t m_span = 0, m_a = 0, m_b = 0;     // this lane's window of the batch
+    unsigned pending = 0;                      // lanes whose windows are still to be visited
+    auto fetch = [&]() {
+        const int64_t i = batch + lane * step;
+        bool ok = false;
+        if (i < c1) {
+            int64_t lo, hi;
+            if (span_row(c, i, lo, hi) >= 0) {
+                int64_t a, b;
+                range_window(ix.off + (c.first_cell + i) * (ix.n_ranges - 1), r, ix.n_ranges, hi - lo, a, b);
+                m_span = i;
+                m_a = lo + a;
+                m_b = lo + b;
+                ok = true;
+            }
+        }
+        pending = __ballot_sync(kFull, ok);
+    };
+    auto next = [&](Win &w) -> bool {
+        for (;;) {
+            if (pending) {
+                const int j = __ffs(pending) - 1;
+                pending &= pending - 1;
+                w.span = __shfl_sync(kFull, m_span, j);
+                w.a = __shfl_sync(kFull, m_a, j);
+                w.b = __shfl_sync(kFull, m_b, j);
+                return true;
+            }
+            batch += 32 * step;
+            if (batch >= c1) return false;
+            fetch();
+        }
+    };
+    if (batch < c1) fetch();
     Win cur, nxt;
     WinBuf bc, bn;
-    bool have = next_window(c, ix, r, i, c1, step, cur);
+    bool have = next(cur);
     if (have) win_load(c, cur.a, cur.b < cur.a + kSpan ? cur.b : cur.a + kSpan, bc);
     while (have) {
-        const bool hn = next_window(c, ix, r, i, c1, step, nxt);
+        const bool hn = next(nxt);
         if (hn) win_load(c, nxt.a, nxt.b < nxt.a + kSpan ? nxt.b : nxt.a + kSpan, bn);
         cell(cur);
         for (int64_t s = cur.a; s < cur.b; s += kSpan) {
