@@ -733,10 +733,14 @@ int crest_pca_solve(crest_pca *p, int64_t n, int64_t k) {
 int crest_pca_results(crest_pca *p, double *variance, double *loadings, double *total, double *colsum) {
     CREST_REQUIRE(p, CREST_EINVAL, "plan is NULL");
     CREST_TRY(bind_device(p->device));
+    CREST_CUDA_TRY(cudaDeviceSynchronize());  // the plan's streams may be non-blocking
     if (variance && p->k) CREST_CUDA_TRY(cudaMemcpy(variance, p->vals.ptr, 8 * p->k, cudaMemcpyDeviceToHost));
     if (loadings && p->k) CREST_CUDA_TRY(cudaMemcpy(loadings, p->vecs.ptr, 8 * p->d * p->k, cudaMemcpyDeviceToHost));
-    if (total) CREST_CUDA_TRY(cudaMemcpy(total, p->total.ptr, 8, cudaMemcpyDeviceToHost));
-    if (colsum) CREST_CUDA_TRY(cudaMemcpy(colsum, p->colsum.ptr, 8 * p->d, cudaMemcpyDeviceToHost));
+    if (total) {  // the total is reduced by crest_pca_solve; 0 before it
+        *total = 0.0;
+        if (p->total.ptr) CREST_CUDA_TRY(cudaMemcpy(total, p->total.ptr, 8, cudaMemcpyDeviceToHost));
+    }
+    if (colsum && p->d) CREST_CUDA_TRY(cudaMemcpy(colsum, p->colsum.ptr, 8 * p->d, cudaMemcpyDeviceToHost));
     return CREST_OK;
 }
 

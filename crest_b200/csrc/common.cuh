@@ -27,6 +27,7 @@ struct Status {
         if (_e != cudaSuccess) {                                                                \
             ::crest::set_error("CUDA error %s at %s:%d: %s", cudaGetErrorName(_e), __FILE__,    \
                                __LINE__, cudaGetErrorString(_e));                               \
+            (void)cudaGetLastError(); /* a non-sticky error must not fail the next call */      \
             return CREST_ECUDA;                                                                 \
         }                                                                                       \
     } while (0)

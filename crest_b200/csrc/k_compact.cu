@@ -212,11 +212,15 @@ __global__ void __launch_bounds__(kDensifyCWarps * 32) k_densify_compact(
     using E = typename CElem<MODE>::T;
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr bool priv = MODE != 0;
-    double *s_col = reinterpret_cast<double *>(smem);
+    // column sums of the stored entries' scaled values in 32.32 fixed point
+    // (native 64-bit integer shared atomics; exact, so the block's partial
+    // does not depend on the order of the adds); |s| >= 2^20 goes straight
+    // to the f64 global sum
+    long long *s_col = reinterpret_cast<long long *>(smem);
     E *shift_row = reinterpret_cast<E *>(smem + (priv ? sizeof(double) * (size_t)round_up(d, 2) : 0));
     if (priv) {
         for (int64_t j = threadIdx.x; j < d_pad; j += blockDim.x) shift_row[j] = (E)((shift && j < d) ? shift[j] : 0.0);
-        for (int64_t j = threadIdx.x; j < d; j += blockDim.x) s_col[j] = 0.0;
+        for (int64_t j = threadIdx.x; j < d; j += blockDim.x) s_col[j] = 0;
     }
     __syncthreads();
     const int lane = lane_id();
@@ -265,7 +269,11 @@ __global__ void __launch_bounds__(kDensifyCWarps * 32) k_densify_compact(
                     row[sub] = h;
                     row_lo[sub] = l;
                 }
-                atomicAdd(s_col + sub, s);
+                if (fabs(s) < 1048576.0)
+                    atomicAdd(reinterpret_cast<unsigned long long *>(s_col + sub),
+                              (unsigned long long)__double2ll_rn(s * 4294967296.0));
+                else
+                    atomicAdd(colsum + sub, s);
             }
         }
     }
@@ -273,7 +281,7 @@ __global__ void __launch_bounds__(kDensifyCWarps * 32) k_densify_compact(
     if (priv) {
         __syncthreads();
         for (int64_t j = threadIdx.x; j < d; j += blockDim.x)
-            if (s_col[j] != 0.0) atomicAdd(colsum + j, s_col[j]);
+            if (s_col[j] != 0) atomicAdd(colsum + j, (double)s_col[j] * 0x1.0p-32);
     }
 }
 
@@ -288,8 +296,9 @@ static int densify_compact_t(const int64_t *indptr, int64_t cell0, int64_t n, co
     int per_sm = 0;
     CREST_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_densify_compact<MODE>,
                                                                  kDensifyCWarps * 32, smem));
+    // at most two blocks per SM: each block flushes its column sums once
     const int64_t blocks =
-        std::min<int64_t>(ceil_div(m_pad, kDensifyCWarps), (int64_t)device_sms() * std::max(per_sm, 1));
+        std::min<int64_t>(ceil_div(m_pad, kDensifyCWarps), (int64_t)device_sms() * std::min(std::max(per_sm, 1), 2));
     k_densify_compact<MODE><<<(unsigned)blocks, kDensifyCWarps * 32, smem, st>>>(
         indptr, cell0, n, in, target_sum, log1p, t, shift, w.d, w.d_pad, m_pad, w.tile, w.colsum_chunk, w.n_kept);
     CREST_CUDA_TRY(cudaGetLastError());

@@ -222,12 +222,219 @@ __global__ void k_gemm_reduce(Gemm g, int ksplit, const double *__restrict__ ws)
     g.O[o] = v;
 }
 
+// Tall-skinny products O = alpha op(A) B + beta X + gamma Y with B (K x N,
+// N <= 64) column-major and op(A) = A (M x K) or A^T (A given K x M), all
+// column-major (the filter and Rayleigh-Ritz products C V and V^T W of the
+// subspace iteration): FP64 tensor-core MMAs (m8n8k4).
+//
+// CTA tile 64 x BN (BN = 16 NF), eight warps as 4 (M) x 2 (N), each warp
+// 16 x 8 NF outputs = 2 x NF fragments of 8 x 8.  K in steps of 16 through a
+// three-stage cp.async ring; shared-memory rows are padded so that each
+// half-warp's 8-byte fragment loads fall in 16 distinct 8-byte slots (row
+// strides of 68 and 20 doubles are 4 mod 16; op(A) = A^T is staged [m][k]
+// like B).  K is split over gridDim.z (about
+// two CTAs per SM); each slice writes its partial tile to ws, and the last
+// slice to finish (a per-tile arrival counter) sums all slices in slice order
+// and applies the epilogue, so results do not depend on scheduling.
+namespace dm {
+constexpr int kBM = 64, kBK = 16, kStages = 3, kThreads = 256;
+constexpr int kAS = kBM + 4;  // A stage: [k][m], m stride 68
+constexpr int kBS = kBK + 4;  // B stage: [n][k], k stride 20
+constexpr int kAStage = kBM * kBS > kBK * kAS ? kBM * kBS : kBK * kAS, kBStage = 64 * kBS;
+constexpr size_t kSmem = sizeof(double) * (size_t)kStages * (kAStage + kBStage);
+constexpr int kMaxTiles = 1024;
+
+__device__ __forceinline__ void cp16(void *smem, const void *gmem, bool ok) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int n = ok ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(c[0]), "+d"(c[1])
+                 : "d"(a), "d"(b));
+}
+
+template <int NF, bool TA>
+__global__ void __launch_bounds__(kThreads, 2) k_gemm_dmma(Gemm g, int kchunk, double *__restrict__ ws,
+                                                           int *__restrict__ cnt) {
+    constexpr int BN = 16 * NF;
+    extern __shared__ __align__(16) double sm[];
+    double *As = sm, *Bs = sm + kStages * kAStage;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp & 3, wn = warp >> 2;
+    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN;
+    const int kb = blockIdx.z * kchunk, ke = min(g.K, kb + kchunk);
+    const int ntiles = (ke - kb + kBK - 1) / kBK;
+
+    auto load = [&](int t, int stage) {
+        const int k0 = kb + t * kBK;
+        double *as = As + stage * kAStage, *bs = Bs + stage * kBStage;
+        // A: 16 k x 64 m = 512 chunks of two m ([k][m]), or of two k for A^T ([m][k])
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int c = tid + r * kThreads;
+            if (!TA) {
+                const int kk = c >> 5, mm = (c & 31) * 2;
+                const int m = m0 + mm, k = k0 + kk;
+                const bool ok = m < g.M && k < ke;
+                cp16(as + kk * kAS + mm, ok ? g.A + m + (int64_t)k * g.lda : g.A, ok);
+            } else {
+                const int mm = c >> 3, kk = (c & 7) * 2;
+                const int m = m0 + mm, k = k0 + kk;
+                const bool ok = m < g.M && k < ke;
+                cp16(as + mm * kBS + kk, ok ? g.A + k + (int64_t)m * g.lda : g.A, ok);
+            }
+        }
+        // B: BN n x 16 k = 8 BN chunks of two k
+        for (int c = tid; c < 8 * BN; c += kThreads) {
+            const int nn = c >> 3, kk = (c & 7) * 2;
+            const int n = n0 + nn, k = k0 + kk;
+            const bool ok = n < g.N && k < ke;
+            cp16(bs + nn * kBS + kk, ok ? g.B + k + (int64_t)n * g.ldb : g.B, ok);
+        }
+    };
+
+    double acc[2][NF][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < NF; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+#pragma unroll
+    for (int s = 0; s < kStages - 1; ++s) {
+        if (s < ntiles) load(s, s);
+        cp_commit();
+    }
+    const int ar = lane >> 2, ac = lane & 3;  // fragment row / column of this lane
+    for (int t = 0; t < ntiles; ++t) {
+        cp_wait<kStages - 2>();
+        __syncthreads();
+        if (t + kStages - 1 < ntiles) load(t + kStages - 1, (t + kStages - 1) % kStages);
+        cp_commit();
+        const double *as = As + (t % kStages) * kAStage + (TA ? (wm * 16 + ar) * kBS + ac : wm * 16 + ar + ac * kAS);
+        const double *bs = Bs + (t % kStages) * kBStage + (wn * 8 * NF + ar) * kBS + ac;
+#pragma unroll
+        for (int k4 = 0; k4 < kBK; k4 += 4) {
+            double a[2], b[NF];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) a[i] = TA ? as[i * 8 * kBS + k4] : as[k4 * kAS + i * 8];
+#pragma unroll
+            for (int j = 0; j < NF; ++j) b[j] = bs[j * 8 * kBS + k4];
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < NF; ++j) dmma(acc[i][j], a[i], b[j]);
+        }
+    }
+    cp_wait<0>();
+
+    constexpr int R = 4 * NF;  // partial values per thread
+    const int tile = blockIdx.x + gridDim.x * blockIdx.y;
+    if (gridDim.z > 1) {
+        double *part = ws + ((int64_t)tile * gridDim.z + blockIdx.z) * R * kThreads + tid;
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < NF; ++j)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) __stcg(part + ((i * NF + j) * 2 + h) * kThreads, acc[i][j][h]);
+        __threadfence();
+        __syncthreads();
+        __shared__ int last;
+        if (tid == 0) last = atomicAdd(cnt + tile, 1) == (int)gridDim.z - 1;
+        __syncthreads();
+        if (!last) return;
+        __threadfence();
+        const double *base = ws + (int64_t)tile * gridDim.z * R * kThreads + tid;
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < NF; ++j)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    double s = 0.0;
+                    for (int z = 0; z < (int)gridDim.z; ++z)
+                        s += __ldcg(base + ((int64_t)z * R + (i * NF + j) * 2 + h) * kThreads);
+                    acc[i][j][h] = s;
+                }
+        if (tid == 0) cnt[tile] = 0;  // ready for the next product
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < NF; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int m = m0 + wm * 16 + i * 8 + ar, n = n0 + wn * 8 * NF + j * 8 + ac * 2 + h;
+                if (m >= g.M || n >= g.N) continue;
+                const int64_t o = m + (int64_t)n * g.ldo;
+                double v = g.alpha * acc[i][j][h];
+                if (g.X) v += g.beta * g.X[o];
+                if (g.Y) v += g.gamma * g.Y[o];
+                g.O[o] = v;
+            }
+}
+}  // namespace dm
+
 struct GemmWs {
-    DevBuf ws;
+    DevBuf ws, dws, cnt;
 };
+
+static bool dmma_enabled() {  // CREST_EIG_DMMA=0: CUDA-core kernel for every product
+    static const bool on = [] {
+        const char *e = getenv("CREST_EIG_DMMA");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+static bool dmma_fits(const Gemm &g) {
+    auto al = [](const void *p) { return ((uintptr_t)p & 15) == 0; };
+    return !g.tB && g.N >= 1 && g.N <= 64 && g.M >= 1 && g.K >= dm::kBK && !(g.K & 1) && !(g.lda & 1) &&
+           !(g.ldb & 1) && (g.tA || !(g.M & 1)) && al(g.A) && al(g.B);
+}
+
+template <int NF>
+static int launch_dmma(const Gemm &g, dim3 grid, int kchunk, double *ws, int *cnt, cudaStream_t st) {
+    if (g.tA) {
+        CREST_TRY(ensure_smem_attr((const void *)dm::k_gemm_dmma<NF, true>, dm::kSmem));
+        dm::k_gemm_dmma<NF, true><<<grid, dm::kThreads, dm::kSmem, st>>>(g, kchunk, ws, cnt);
+    } else {
+        CREST_TRY(ensure_smem_attr((const void *)dm::k_gemm_dmma<NF, false>, dm::kSmem));
+        dm::k_gemm_dmma<NF, false><<<grid, dm::kThreads, dm::kSmem, st>>>(g, kchunk, ws, cnt);
+    }
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
+}
+
+static int gemm_dmma(const Gemm &g, GemmWs &w, cudaStream_t st) {
+    const int nf = g.N <= 16 ? 1 : g.N <= 32 ? 2 : 4;
+    const int mt = (int)ceil_div(g.M, dm::kBM), nt = (int)ceil_div(g.N, 16 * nf);
+    int ks = std::max(1, std::min((2 * device_sms()) / (mt * nt), g.K / (4 * dm::kBK)));
+    const int kchunk = (int)round_up(ceil_div(g.K, ks), dm::kBK);
+    ks = (int)ceil_div(g.K, kchunk);
+    CREST_REQUIRE(mt * nt <= dm::kMaxTiles, CREST_EINVAL, "GEMM too large for the tile counters");
+    if (!w.cnt.ptr) {
+        CREST_TRY(w.cnt.ensure(sizeof(int) * dm::kMaxTiles));
+        CREST_CUDA_TRY(cudaMemsetAsync(w.cnt.ptr, 0, sizeof(int) * dm::kMaxTiles, st));
+    }
+    if (ks > 1) CREST_TRY(w.dws.ensure(sizeof(double) * (size_t)mt * nt * ks * 4 * nf * dm::kThreads));
+    const dim3 grid(mt, nt, ks);
+    double *ws = w.dws.as<double>();
+    int *cnt = w.cnt.as<int>();
+    if (nf == 1) return launch_dmma<1>(g, grid, kchunk, ws, cnt, st);
+    if (nf == 2) return launch_dmma<2>(g, grid, kchunk, ws, cnt, st);
+    return launch_dmma<4>(g, grid, kchunk, ws, cnt, st);
+}
 
 int gemm(const Gemm &g, GemmWs &w, cudaStream_t st) {
     prof::Scope ps("eig_gemm_fp64", st);
+    if (dmma_fits(g) && dmma_enabled()) return gemm_dmma(g, w, st);
     const int mt = (int)ceil_div(g.M, kGM), nt = (int)ceil_div(g.N, kGN);
     int ksplit = 1;
     if (g.K > 0) {  // about one CTA per SM, slices of at least 64
@@ -298,7 +505,7 @@ __global__ void __launch_bounds__(512) k_jacobi(const double *__restrict__ Ain, 
     }
     __syncthreads();
     const int half = n / 2;
-    const double eps = (double)n * 0x1.0p-52;
+    const double eps = (double)n * 0x1.0p-52, eps2 = eps * eps;
     int sweep = 0;
     for (; sweep < max_sweeps; ++sweep) {
         for (int r = 0; r < n - 1; ++r) {
@@ -308,10 +515,13 @@ __global__ void __launch_bounds__(512) k_jacobi(const double *__restrict__ Ain, 
                 const int p = a < b ? a : b, q = a < b ? b : a;
                 const double apq = S[p + q * ld], app = S[p + p * ld], aqq = S[q + q * ld];
                 double c = 1.0, s = 0.0;
-                if (fabs(apq) > fmax(eps * sqrt(fabs(app * aqq)), floor_abs)) {
-                    const double tau = (aqq - app) / (2.0 * apq);
-                    const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-                    c = 1.0 / sqrt(1.0 + t * t);
+                if (fabs(apq) > floor_abs && apq * apq > eps2 * fabs(app * aqq)) {
+                    // t = sign(tau) / (|tau| + sqrt(1 + tau^2)), tau = (aqq - app) / (2 apq),
+                    // written with one square root and one division
+                    const double dd = aqq - app, two = 2.0 * apq;
+                    const double r = sqrt(fma(dd, dd, two * two));
+                    const double t = (dd >= 0.0 ? two : -two) / (fabs(dd) + r);
+                    c = rsqrt(fma(t, t, 1.0));
                     s = t * c;
                     rotated = 1;
                 }
@@ -775,6 +985,140 @@ __global__ void __launch_bounds__(1024) k_lanczos_step(double *V, int64_t d, int
     }
 }
 
+// All L Lanczos steps in one cooperative launch (one CTA per SM, rows of C
+// and of the basis split evenly over the CTAs).  Per step, three grid
+// barriers:
+//   1. w' = C v_j / beta_{j-1} on this CTA's rows (v_j = w / beta_{j-1}
+//      is normalised on the fly; row i of C is its column i), and the
+//      partial dots of those rows with v_0..v_j;
+//   2. h = the sum of the partials in CTA order; w' -= V h on this CTA's
+//      rows, and the partials of the second Gram-Schmidt pass;
+//   3. the same subtraction again, and the partial squared norm.
+// alpha_j is the first-pass coefficient of v_j.  All sums run in a fixed
+// order, so the run is deterministic.  Each barrier wait is bounded (about
+// one second of %globaltimer); on expiry the CTA raises *err and every later
+// barrier is skipped, so the launch always ends.
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ void grid_barrier(unsigned *bar, unsigned nblk, int *err) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = bar + 1;
+        volatile int *e = err;
+        if (!*e) {
+            const unsigned g = *gen;
+            __threadfence();
+            if (atomicAdd(bar, 1u) == nblk - 1) {
+                atomicExch(bar, 0u);
+                __threadfence();
+                atomicAdd(bar + 1, 1u);
+            } else {
+                const unsigned long long t0 = gtimer();
+                while (*gen == g) {
+                    if (*e || gtimer() - t0 > 1000000000ull) {
+                        atomicExch(err, 1);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+struct LanczosArgs {
+    const double *C;
+    int64_t d;
+    int L;
+    double *Z;     // d x (kLanczos + 1), column 0 = the normalised start vector
+    double *w[2];  // d each
+    double *part;  // gridDim.x x 3 x (kLanczos + 1)
+    double *ab;    // alpha [0, kLanczos), beta [kLanczos, 2 kLanczos)
+    unsigned *bar;
+    int *err;
+};
+
+__global__ void __launch_bounds__(512) k_lanczos(LanczosArgs a) {
+    constexpr int P = kLanczos + 1;
+    __shared__ double coef[P];
+    __shared__ double scal;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+    const unsigned nb = gridDim.x, b = blockIdx.x;
+    const int64_t d = a.d, r0 = d * b / nb, r1 = d * (b + 1) / nb;
+    double *part = a.part + (size_t)b * 3 * P;
+    // the start vector plays the role of w with beta = 1
+    for (int64_t r = r0 + tid; r < r1; r += nt) a.w[1][r] = a.Z[r];
+    if (tid == 0) scal = 1.0;
+    grid_barrier(a.bar, nb, a.err);
+    for (int j = 0; j < a.L; ++j) {
+        const double *win = a.w[(j + 1) & 1];
+        double *wout = a.w[j & 1];
+        const double inv = 1.0 / scal;  // 1 / beta_{j-1}
+        double *vj = a.Z + (int64_t)j * d;
+        for (int64_t r = r0 + tid; r < r1; r += nt) vj[r] = win[r] * inv;
+        for (int64_t r = r0 + wid; r < r1; r += nw) {  // row r of C = column r
+            const double *col = a.C + r * d;
+            double t = 0.0;
+            for (int64_t i = lane; i < d; i += 32) t += col[i] * win[i];
+            for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            if (lane == 0) wout[r] = t * inv;
+        }
+        __syncthreads();
+        for (int pass = 0; pass < 3; ++pass) {
+            double *pp = part + pass * P;
+            if (pass < 2) {  // partial dots of this CTA's rows with v_0..v_j
+                for (int i = wid; i <= j; i += nw) {
+                    const double *zi = a.Z + (int64_t)i * d;
+                    double t = 0.0;
+                    for (int64_t r = r0 + lane; r < r1; r += 32) t += zi[r] * wout[r];
+                    for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+                    if (lane == 0) pp[i] = t;
+                }
+            } else {
+                double t = 0.0;
+                for (int64_t r = r0 + tid; r < r1; r += nt) t += wout[r] * wout[r];
+                for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+                if (lane == 0) coef[wid] = t;
+                __syncthreads();
+                if (tid == 0) {
+                    double s = 0.0;
+                    for (int i = 0; i < nw; ++i) s += coef[i];
+                    pp[0] = s;
+                }
+            }
+            grid_barrier(a.bar, nb, a.err);
+            if (pass == 2) break;
+            for (int i = tid; i <= j; i += nt) {  // coefficients, summed in CTA order
+                double s = 0.0;
+                for (unsigned c = 0; c < nb; ++c) s += __ldcg(a.part + ((size_t)c * 3 + pass) * P + i);
+                coef[i] = s;
+            }
+            __syncthreads();
+            if (pass == 0 && b == 0 && tid == 0) a.ab[j] = coef[j];
+            for (int64_t r = r0 + tid; r < r1; r += nt) {
+                double v = wout[r];
+                for (int i = 0; i <= j; ++i) v -= coef[i] * a.Z[(int64_t)i * d + r];
+                wout[r] = v;
+            }
+            __syncthreads();
+        }
+        if (tid == 0) {
+            double s = 0.0;
+            for (unsigned c = 0; c < nb; ++c) s += __ldcg(a.part + ((size_t)c * 3 + 2) * P);
+            const double beta = sqrt(s);
+            scal = beta > 0.0 ? beta : 1.0;
+            if (b == 0) a.ab[kLanczos + j] = beta;
+        }
+        __syncthreads();
+    }
+}
+
 // Lanczos tridiagonal T (L x L, col-major) from alpha = ab[0..L), beta = ab[kLanczos..).
 __global__ void k_tridiag(const double *ab, int L, double *T) {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -784,9 +1128,38 @@ __global__ void k_tridiag(const double *ab, int L, double *T) {
 }
 
 struct EigWork {
-    DevBuf C, Cs, V, W, Y0, Y1, H, Q, vals, sorted, perm, scal, lz, lw, lab, res, rinv, fail;
+    DevBuf C, Cs, V, W, Y0, Y1, H, Q, vals, sorted, perm, scal, lz, lw, lw2, lpart, lbar, lab, res, rinv, fail;
     GemmWs g;
 };
+
+// The cooperative Lanczos launch; CREST_ERUNTIME (nothing launched) when the
+// device cannot hold one CTA per SM of it.
+int lanczos_coop(EigWork &w, const double *C, int64_t d, int L, cudaStream_t st) {
+    static const bool off = [] {
+        const char *e = getenv("CREST_EIG_COOP");
+        return e && e[0] == '0';
+    }();
+    if (off) return CREST_ERUNTIME;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lanczos, 512, 0) != cudaSuccess || per_sm < 1) {
+        (void)cudaGetLastError();
+        return CREST_ERUNTIME;
+    }
+    const int nb = (int)std::min<int64_t>(device_sms(), std::max<int64_t>(1, d / 4));
+    CREST_TRY(w.lw2.ensure(sizeof(double) * (size_t)d));
+    CREST_TRY(w.lpart.ensure(sizeof(double) * (size_t)nb * 3 * (kLanczos + 1)));
+    CREST_TRY(w.lbar.ensure(sizeof(unsigned) * 2));
+    CREST_CUDA_TRY(cudaMemsetAsync(w.lbar.ptr, 0, sizeof(unsigned) * 2, st));
+    CREST_CUDA_TRY(cudaMemsetAsync(w.fail.as<int>() + 3, 0, sizeof(int), st));
+    LanczosArgs a{C, d, L, w.lz.as<double>(), {w.lw.as<double>(), w.lw2.as<double>()}, w.lpart.as<double>(),
+                  w.lab.as<double>(), w.lbar.as<unsigned>(), w.fail.as<int>() + 3};
+    void *args[] = {&a};
+    if (cudaLaunchCooperativeKernel((const void *)k_lanczos, dim3(nb), dim3(512), args, 0, st) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return CREST_ERUNTIME;
+    }
+    return CREST_OK;
+}
 
 // Orthonormalise columns [j0, j0+q) of the d x p block Y against its first
 // j0 columns (already orthonormal) and among themselves: shifted Cholesky QR
@@ -918,9 +1291,11 @@ int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_
         const int L = (int)std::min<int64_t>(kLanczos, d - 1);
         {
             prof::Scope ps("eig_lanczos", st);
-            for (int j = 0; j < L; ++j) {
-                k_symv<<<(unsigned)ceil_div(d * 32, 256), 256, 0, st>>>(C, d, LZ + (int64_t)j * d, lw);
-                k_lanczos_step<<<1, 1024, 0, st>>>(LZ, d, j, lw, lab);
+            if (lanczos_coop(w, C, d, L, st) != CREST_OK) {  // one launch per step instead
+                for (int j = 0; j < L; ++j) {
+                    k_symv<<<(unsigned)ceil_div(d * 32, 256), 256, 0, st>>>(C, d, LZ + (int64_t)j * d, lw);
+                    k_lanczos_step<<<1, 1024, 0, st>>>(LZ, d, j, lw, lab);
+                }
             }
         }
         CREST_CUDA_TRY(cudaGetLastError());
@@ -932,7 +1307,10 @@ int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_
         CREST_CUDA_TRY(cudaMemcpyAsync(hab.data(), lab, sizeof(double) * 2 * kLanczos, cudaMemcpyDeviceToHost, st));
         CREST_CUDA_TRY(cudaMemcpyAsync(tw.data(), jvals, sizeof(double) * L, cudaMemcpyDeviceToHost, st));
         CREST_CUDA_TRY(cudaMemcpyAsync(tz.data(), Q, sizeof(double) * L * L, cudaMemcpyDeviceToHost, st));
+        int lz_err = 0;
+        CREST_CUDA_TRY(cudaMemcpyAsync(&lz_err, w.fail.as<int>() + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
         CREST_CUDA_TRY(cudaStreamSynchronize(st));
+        CREST_REQUIRE(!lz_err, CREST_ERUNTIME, "Lanczos grid barrier timed out");
         int imin = 0, imax = 0;
         for (int i = 1; i < L; ++i) {
             if (tw[i] < tw[imin]) imin = i;

@@ -668,17 +668,34 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_pair(const __grid_constant
             const bool corr = half == 0 && a.bias;
             double *G = half == 0 ? a.G : a.G_aux;
             const double nk = (double)*a.n_kept;
-            for (int r = e; r < kHalfRows; r += kEpiWarps) {
-                const int64_t ga = (int64_t)bi * kN + (int64_t)rank * kHalfRows + r;
-                if (ga >= a.d) break;
-                const double ba = corr ? a.bias[ga] : 0.0, ca = corr ? a.colsum[ga] : 0.0;
-                double *grow = G + ga * a.d;
-                for (int cc = lane; cc < kN; cc += 32) {
-                    const int64_t gb = (int64_t)bj * kN + cc;
-                    if (gb >= a.d || gb < ga) continue;
-                    double v = (double)stage[r * kPitch + cc];
-                    if (corr) v = v - ba * a.colsum[gb] - ca * a.bias[gb] - nk * ba * a.bias[gb];
-                    grow[gb] += v;
+            // two rows per pass, every load of a pass issued before the
+            // first add: 16 independent G reads in flight per lane
+            for (int r0 = e; r0 < kHalfRows; r0 += 2 * kEpiWarps) {
+                double gv[2][8];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int64_t ga = (int64_t)bi * kN + (int64_t)rank * kHalfRows + r0 + u * kEpiWarps;
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        const int64_t gb = (int64_t)bj * kN + lane + 32 * c;
+                        gv[u][c] = (ga < a.d && gb < a.d && gb >= ga) ? G[ga * a.d + gb] : 0.0;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int r = r0 + u * kEpiWarps;
+                    const int64_t ga = (int64_t)bi * kN + (int64_t)rank * kHalfRows + r;
+                    if (ga >= a.d) continue;
+                    const double ba = corr ? a.bias[ga] : 0.0, ca = corr ? a.colsum[ga] : 0.0;
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) {
+                        const int cc = lane + 32 * c;
+                        const int64_t gb = (int64_t)bj * kN + cc;
+                        if (gb >= a.d || gb < ga) continue;
+                        double v = (double)stage[r * kPitch + cc];
+                        if (corr) v = v - ba * a.colsum[gb] - ca * a.bias[gb] - nk * ba * a.bias[gb];
+                        G[ga * a.d + gb] = gv[u][c] + v;
+                    }
                 }
             }
         }
