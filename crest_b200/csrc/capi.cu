@@ -42,6 +42,36 @@ static bool injected_alloc_failure() {
     return --countdown == 0;
 }
 
+// The library's memory pool of the current device (nullptr: none).
+static cudaMemPool_t device_pool() {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64];
+    static bool tried[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!tried[dev]) {
+        tried[dev] = true;
+        int supported = 0;
+        cudaDeviceGetAttribute(&supported, cudaDevAttrMemoryPoolsSupported, dev);
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        if (supported && cudaMemPoolCreate(&pool, &props) == cudaSuccess) {
+            uint64_t keep = ~(uint64_t)0;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            pools[dev] = pool;
+        }
+        cudaGetLastError();
+    }
+    return pools[dev];
+}
+
 int DevBuf::ensure(size_t bytes) {
     if (bytes <= cap && ptr) return CREST_OK;
     release();
@@ -50,8 +80,16 @@ int DevBuf::ensure(size_t bytes) {
         set_error("device allocation of %zu bytes failed: out of memory (injected)", want);
         return CREST_ENOMEM;
     }
-    cudaError_t e = cudaMalloc(&ptr, want);
+    cudaMemPool_t pool = device_pool();
+    cudaError_t e;
+    if (pool) {  // ordered on the legacy stream, which is idle here: usable on every stream after the sync
+        e = cudaMallocFromPoolAsync(&ptr, want, pool, 0);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    } else {
+        e = cudaMalloc(&ptr, want);
+    }
     if (e != cudaSuccess) {
+        if (ptr && pool) cudaFreeAsync(ptr, 0);
         ptr = nullptr;
         cap = 0;
         cudaGetLastError();
@@ -59,12 +97,22 @@ int DevBuf::ensure(size_t bytes) {
         return CREST_ENOMEM;
     }
     cap = want;
+    pooled = pool != nullptr;
     return CREST_OK;
 }
 void DevBuf::release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) {
+        if (pooled) {  // as cudaFree: the device is idle before the memory goes back to the pool
+            cudaDeviceSynchronize();
+            cudaFreeAsync(ptr, 0);
+            cudaStreamSynchronize(0);
+        } else {
+            cudaFree(ptr);
+        }
+    }
     ptr = nullptr;
     cap = 0;
+    pooled = false;
 }
 int HostBuf::ensure(size_t bytes) {
     if (bytes <= cap && ptr) return CREST_OK;

@@ -1,6 +1,8 @@
 // Device-resident matrix and PCA plan (layer 2 of the C ABI).
 //
-// The matrix is either copied to HBM once (residency DEVICE) or streamed
+// The matrix is either copied to HBM once (residency DEVICE; in chunks of
+// whole cells on a copy stream, the Gram pass consuming each chunk as it
+// arrives) or streamed
 // from host memory in fixed cell chunks through two device buffers on a copy
 // stream, the copy of chunk i+1 overlapping the kernels of chunk i
 // (residency HOST; the reference's out-of-core model, crest/core.py:54-62 and
@@ -25,6 +27,13 @@ struct crest_matrix {
     bool registered = false;
     crest::DevBuf d_indptr, d_indices, d_data;
     cudaStream_t compute = nullptr, copy = nullptr;
+    // device residency: the CSR arrays are copied in chunks of whole cells on
+    // the copy stream; chunk u covers cells [up_end[u-1], up_end[u]) and is on
+    // the device once up_ev[u] has completed.  up_waited: the compute stream
+    // already waits for every chunk.
+    std::vector<int64_t> up_end;
+    std::vector<cudaEvent_t> up_ev;
+    bool up_waited = true;
     crest::DevBuf buf_idx[2], buf_val[2];
     cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
     // per-pass staging
@@ -68,6 +77,16 @@ struct crest_pca {
 
 namespace crest {
 namespace {
+
+constexpr int64_t kUploadCells = 131072;  // cells per upload chunk (a multiple of the Gram tile)
+
+// The compute stream waits for every upload chunk (once per matrix).
+int wait_upload(crest_matrix *m) {
+    if (m->up_waited || m->up_ev.empty()) return CREST_OK;
+    CREST_CUDA_TRY(cudaStreamWaitEvent(m->compute, m->up_ev.back(), 0));
+    m->up_waited = true;
+    return CREST_OK;
+}
 
 struct Timer {
     cudaEvent_t a = nullptr, b = nullptr;
@@ -274,6 +293,8 @@ int compact_pass(crest_matrix *m, const DevChunk &proto, int64_t d, bool &done, 
     done = false;
     m->cmp_valid = false;
     if (m->residency != CREST_MEM_DEVICE || m->compact_off || m->n_cells == 0) return CREST_OK;
+    // the extract kernel keeps one class byte per gene in shared memory
+    if (4 * gene_class_words(std::max<int64_t>(m->n_genes, 1)) > (size_t)kMaxSmem) return CREST_OK;
     const size_t nnz = (size_t)std::max<int64_t>(m->nnz, 1), n = (size_t)m->n_cells;
     if (m->cmp_code.ensure(4 * nnz) || m->cmp_x.ensure(4 * nnz) || m->cmp_n.ensure(4 * n) ||
         m->cmp_scale.ensure(8 * n) || m->cmp_status.ensure(sizeof(int)) ||
@@ -286,15 +307,21 @@ int compact_pass(crest_matrix *m, const DevChunk &proto, int64_t d, bool &done, 
     }
     CREST_TRY(launch_gene_class(m->code.as<int32_t>(), m->n_genes, d, m->cls.as<uint32_t>(), st));
     CREST_CUDA_TRY(cudaMemsetAsync(m->cmp_status.ptr, 0, sizeof(int), st));
+    done = true;
+    return CREST_OK;
+}
+
+// Compact form of cells [c0, c1) (after compact_pass), once the upload
+// chunk(s) holding them are on the device.
+int compact_extract(crest_matrix *m, const DevChunk &proto, int64_t d, int64_t c0, int64_t c1, cudaStream_t st) {
     DevChunk c = proto;
     c.genes = m->d_indices.as<uint32_t>();
     c.values = m->d_data.as<float>();
-    c.first_cell = 0;
+    c.span_ptr = m->d_indptr.as<int64_t>() + c0;
+    c.first_cell = (uint32_t)c0;
     c.base = 0;
-    c.n_spans = m->n_cells;
-    CREST_TRY(launch_extract(c, m->cls.as<uint32_t>(), m->code.as<int32_t>(), d, compact_view(m), st));
-    done = true;
-    return CREST_OK;
+    c.n_spans = c1 - c0;
+    return launch_extract(c, m->cls.as<uint32_t>(), m->code.as<int32_t>(), d, compact_view(m), st);
 }
 
 // Duplicate-column check of the compact form: only cells whose columns were
@@ -389,9 +416,35 @@ int crest_matrix_create(crest_matrix **out, const int64_t *indptr, const uint32_
     int rc = upload(m->d_indptr, indptr, n_cells + 1, m->compute);
     if (rc) return fail(rc);
     if (residency == CREST_MEM_DEVICE) {
-        rc = upload(m->d_indices, indices, nnz, m->compute);
-        if (!rc) rc = upload(m->d_data, data, nnz, m->compute);
+        // chunked copies on the copy stream, left running: the Gram pass
+        // extracts each chunk as soon as it has arrived (the caller's arrays
+        // must stay valid until the first operation on the matrix returns)
+        rc = m->d_indices.ensure(4 * (size_t)std::max<int64_t>(nnz, 1));
+        if (!rc) rc = m->d_data.ensure(4 * (size_t)std::max<int64_t>(nnz, 1));
         if (rc) return fail(rc);
+        for (int64_t c0 = 0; c0 < n_cells || (c0 == 0 && n_cells == 0); c0 += kUploadCells) {
+            const int64_t c1 = std::min(n_cells, c0 + kUploadCells), e0 = indptr[c0], e1 = indptr[c1];
+            if (e1 > e0) {
+                if (cudaMemcpyAsync(m->d_indices.as<uint32_t>() + e0, indices + e0, 4 * (size_t)(e1 - e0),
+                                    cudaMemcpyHostToDevice, m->copy) != cudaSuccess ||
+                    cudaMemcpyAsync(m->d_data.as<float>() + e0, data + e0, 4 * (size_t)(e1 - e0),
+                                    cudaMemcpyHostToDevice, m->copy) != cudaSuccess) {
+                    set_error("matrix upload failed: %s", cudaGetErrorString(cudaGetLastError()));
+                    return fail(CREST_ECUDA);
+                }
+            }
+            cudaEvent_t ev = nullptr;
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventRecord(ev, m->copy) != cudaSuccess) {
+                if (ev) cudaEventDestroy(ev);
+                set_error("matrix upload failed: %s", cudaGetErrorString(cudaGetLastError()));
+                return fail(CREST_ECUDA);
+            }
+            m->up_ev.push_back(ev);
+            m->up_end.push_back(c1);
+            if (n_cells == 0) break;
+        }
+        m->up_waited = false;
     } else {
         m->h_indices = indices;
         m->h_data = data;
@@ -431,6 +484,8 @@ int crest_matrix_free(crest_matrix *m) {
         if (m->ev_ready[i]) cudaEventDestroy(m->ev_ready[i]);
         if (m->ev_free[i]) cudaEventDestroy(m->ev_free[i]);
     }
+    for (cudaEvent_t ev : m->up_ev) cudaEventDestroy(ev);
+    m->up_ev.clear();
     for (auto *b : {&m->cell_map, &m->gene_map, &m->flag, &m->sub_map, &m->mean, &m->std_, &m->bias, &m->range_off,
                     &m->status, &m->totals})
         b->release();
@@ -455,6 +510,7 @@ int crest_matrix_qc(crest_matrix *m, const int64_t *cell_map, const int32_t *gen
                     uint32_t *gene_ncells, double *gene_total) {
     CREST_REQUIRE(m, CREST_EINVAL, "matrix is NULL");
     CREST_TRY(bind_device(m->device));
+    CREST_TRY(wait_upload(m));
     CREST_TRY(stage_maps(m, cell_map, gene_map, n_rows, n_vars));
     cudaStream_t st = m->compute;
     CREST_TRY(upload(m->flag, flag, n_vars, st));
@@ -512,6 +568,7 @@ int crest_matrix_gene_stats(crest_matrix *m, const int64_t *cell_map, const int3
                             int32_t log1p, int64_t n_vars, double *out) {
     CREST_REQUIRE(m && out, CREST_EINVAL, "NULL argument");
     CREST_TRY(bind_device(m->device));
+    CREST_TRY(wait_upload(m));
     CREST_TRY(stage_maps(m, cell_map, gene_map, -1, n_vars));
     cudaStream_t st = m->compute;
     CREST_TRY(zeros<double>(m->out[0], n_vars * 5, st));
@@ -549,6 +606,7 @@ int crest_matrix_group_gene_sums(crest_matrix *m, const int64_t *cell_map, const
                                  int64_t n_vars, const double *clip, double *sum, double *sumsq, double *nnz) {
     CREST_REQUIRE(m && sum && n_groups >= 0, CREST_EINVAL, "NULL argument");
     CREST_TRY(bind_device(m->device));
+    CREST_TRY(wait_upload(m));
     int64_t n_rows = 0;
     for (int64_t i = 0; i < m->n_cells; ++i) n_rows = std::max<int64_t>(n_rows, cell_map[i] + 1);
     CREST_REQUIRE(n_group_rows >= n_rows && (n_group_rows == 0 || group_of_row), CREST_EINVAL,
@@ -647,14 +705,24 @@ int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
     CREST_TRY(gram_status_reset(p->w, st));
     bool compact = false;
     CREST_TRY(compact_pass(m, proto, p->d, compact, st));
-    if (compact) {  // Gram tiles from the compact HVG form
+    if (compact) {  // per upload chunk: its compact HVG form, then its Gram tiles
         const CompactHvg ch = compact_view(m);
-        for (int64_t s0 = 0; s0 < m->n_cells; s0 += p->w.m_cap) {
-            const int64_t n = std::min(p->w.m_cap, m->n_cells - s0);
-            CREST_TRY(launch_densify_compact(m->d_indptr.as<int64_t>(), s0, n, ch, target_sum, log1p, ds, p->w, st));
-            CREST_TRY(launch_syrk_fold(p->w, n, ds, p->gram.as<double>(), p->colsum.as<double>(), st));
+        int64_t u0 = 0;
+        for (size_t u = 0; u < m->up_end.size() && u0 < m->n_cells; ++u) {
+            const int64_t u1 = m->up_end[u];
+            if (!m->up_waited) CREST_CUDA_TRY(cudaStreamWaitEvent(st, m->up_ev[u], 0));
+            CREST_TRY(compact_extract(m, proto, p->d, u0, u1, st));
+            for (int64_t s0 = u0; s0 < u1; s0 += p->w.m_cap) {
+                const int64_t n = std::min(p->w.m_cap, u1 - s0);
+                CREST_TRY(
+                    launch_densify_compact(m->d_indptr.as<int64_t>(), s0, n, ch, target_sum, log1p, ds, p->w, st));
+                CREST_TRY(launch_syrk_fold(p->w, n, ds, p->gram.as<double>(), p->colsum.as<double>(), st));
+            }
+            u0 = u1;
         }
+        m->up_waited = true;
     } else {
+        CREST_TRY(wait_upload(m));
         CREST_TRY(for_each_piece(m, proto, p->w.m_cap, [&](const DevChunk &c) {
             return gram_over_chunk(c, m->code.as<int32_t>(), ds, p->w, p->gram.as<double>(), p->colsum.as<double>(),
                                    st);
@@ -750,6 +818,7 @@ int crest_pca_project(crest_pca *p, crest_matrix *m, const int64_t *cell_map, co
     CREST_REQUIRE(p && m && out, CREST_EINVAL, "NULL argument");
     CREST_REQUIRE(p->k >= 1, CREST_EINVAL, "crest_pca_solve must run before crest_pca_project");
     CREST_TRY(bind_device(m->device));
+    CREST_TRY(wait_upload(m));
     for (int64_t i = 0; i < n_vars; ++i)
         CREST_REQUIRE(sub_map[i] < p->d, CREST_EINVAL, "sub_map must have length n_vars and values < d");
     cudaStream_t st = m->compute;

@@ -47,9 +47,14 @@ struct Status {
     } while (0)
 
 // A device buffer that only grows; used for per-call staging of chunk inputs.
+// Device buffer that only grows.  Memory comes from a per-device
+// stream-ordered pool that keeps what is returned to it (release threshold
+// unbounded), so buffers freed by one call are handed to the next without
+// new page mappings; plain cudaMalloc when no pool can be created.
 struct DevBuf {
     void *ptr = nullptr;
     size_t cap = 0;
+    bool pooled = false;
     int ensure(size_t bytes);
     void release();
     template <class T> T *as() const { return reinterpret_cast<T *>(ptr); }

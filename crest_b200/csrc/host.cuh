@@ -43,7 +43,7 @@ inline int64_t tile_cells_default() {
 
 // A Gram tile workspace sized for d genes.
 struct GramBufs {
-    DevBuf tile, colsum_chunk, n_kept, shift, status, aux;
+    DevBuf tile, colsum_chunk, n_kept, shift, status, aux, colsum_part;
     int ensure(GramWork &w, int64_t d, int precision, int64_t m_cap) {
         w.d = d;
         // the tensor-core SYRK works on 256 x 256 blocks (pairs of SMs)
@@ -63,6 +63,9 @@ struct GramBufs {
         w.shift = shift.as<double>();
         w.status = status.as<int>();
         w.gram_aux = nullptr;
+        w.colsum_rows = 2 * (int64_t)device_sms();
+        CREST_TRY(colsum_part.ensure(sizeof(long long) * (size_t)w.colsum_rows * (size_t)w.d_pad));
+        w.colsum_part = colsum_part.as<long long>();
         if (precision == CREST_GRAM_BF16X3 && d > 0) {
             const size_t bytes = sizeof(double) * (size_t)d * (size_t)d;
             const bool fresh = aux.cap < bytes;

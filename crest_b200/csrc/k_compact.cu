@@ -26,27 +26,28 @@
 
 namespace crest {
 
-// -------------------------------------------------------- 2-bit classes
-// cls[g >> 4] bits 2 (g & 15) .. +1: bit 0 kept gene, bit 1 HVG column.
+// --------------------------------------------------------- byte classes
+// Byte g of cls: 0 dropped gene, 1 kept gene, 3 HVG column.
 __global__ void k_gene_class(const int32_t *__restrict__ code, int64_t n_gene_map, int64_t d,
                              uint32_t *__restrict__ cls) {
     const int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= ceil_div(n_gene_map, 16)) return;
+    if (w >= ceil_div(n_gene_map, 4)) return;
     uint32_t v = 0;
-    for (int j = 0; j < 16; ++j) {
-        const int64_t g = w * 16 + j;
+    for (int j = 0; j < 4; ++j) {
+        const int64_t g = w * 4 + j;
         if (g >= n_gene_map) break;
         const int32_t m = code[g];
         const uint32_t b = m < 0 ? 0u : (m < d ? 3u : 1u);
-        v |= b << (2 * j);
+        v |= b << (8 * j);
     }
     cls[w] = v;
 }
 
-size_t gene_class_words(int64_t n_gene_map) { return (size_t)round_up(ceil_div(n_gene_map, 16), 4); }
+// words of the table, a multiple of four (whole 16-byte loads)
+size_t gene_class_words(int64_t n_gene_map) { return (size_t)round_up(ceil_div(n_gene_map, 4), 4); }
 
 int launch_gene_class(const int32_t *code, int64_t n_gene_map, int64_t d, uint32_t *cls, cudaStream_t st) {
-    const int64_t nw = ceil_div(n_gene_map, 16);
+    const int64_t nw = ceil_div(n_gene_map, 4);
     if (nw == 0) return CREST_OK;
     k_gene_class<<<(unsigned)ceil_div(nw, 256), 256, 0, st>>>(code, n_gene_map, d, cls);
     CREST_CUDA_TRY(cudaGetLastError());
@@ -56,21 +57,27 @@ int launch_gene_class(const int32_t *code, int64_t n_gene_map, int64_t d, uint32
 // ------------------------------------------------------------- extract
 constexpr int kExtractWarps = 8;
 
+__device__ __forceinline__ int64_t gene_class_words_dev(int64_t n_gene_map) {
+    return round_up(ceil_div(n_gene_map, 4), 4);
+}
+
 template <int DEPTH>
 __global__ void __launch_bounds__(kExtractWarps * 32, 4) k_extract(DevChunk c, const uint32_t *__restrict__ cls,
                                                                 const int32_t *__restrict__ code, int32_t d,
                                                                 CompactHvg out) {
     extern __shared__ __align__(16) uint32_t s_cls[];
-    const int64_t nw = ceil_div(c.n_gene_map, 16);
-    for (int64_t j = threadIdx.x; j < nw; j += blockDim.x) s_cls[j] = __ldg(cls + j);
+    const int64_t n16 = (int64_t)gene_class_words_dev(c.n_gene_map) / 4;
+    for (int64_t j = threadIdx.x; j < n16; j += blockDim.x)
+        reinterpret_cast<uint4 *>(s_cls)[j] = __ldg(reinterpret_cast<const uint4 *>(cls) + j);
     __syncthreads();
+    const uint8_t *s_cls8 = reinterpret_cast<const uint8_t *>(s_cls);
     const int lane = lane_id();
     const int64_t warp = (int64_t)blockIdx.x * kExtractWarps + (threadIdx.x >> 5);
     const int64_t n_warps = (int64_t)gridDim.x * kExtractWarps;
     const bool norm = c.target_sum > 0.0;
     // lookup: -1 dropped gene, -2 kept gene outside the HVG columns, g for an HVG column
     auto lookup = [&](uint32_t g) -> int32_t {
-        const uint32_t b = (s_cls[g >> 4] >> (2 * (g & 15))) & 3u;
+        const uint32_t b = s_cls8[g];
         return b == 0u ? -1 : (b == 1u ? -2 : (int32_t)g);
     };
     bool ordered = true;
@@ -84,7 +91,10 @@ __global__ void __launch_bounds__(kExtractWarps * 32, 4) k_extract(DevChunk c, c
         }
         int32_t *oc = out.code + lo;
         float *ox = out.x + lo;
-        double tsum = 0.0;
+        // kept values summed in FP32 per lane: exact while every value is a
+        // non-negative integer and the lane's sum stays below 2^24 (then all
+        // its partial sums do), which the end of the cell checks
+        float fsum = 0.0f;
         bool integral = true;
         int nq = 0;
         int32_t carry = -1;
@@ -93,9 +103,10 @@ __global__ void __launch_bounds__(kExtractWarps * 32, 4) k_extract(DevChunk c, c
             int32_t col[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                if (m[u] != -1 && norm) {
-                    integral = integral && x[u] == rintf(x[u]) && fabsf(x[u]) < 16777216.0f;
-                    tsum += (double)x[u];
+                if (norm) {
+                    const bool kept = m[u] != -1;
+                    fsum += kept ? x[u] : 0.0f;
+                    integral = integral && (!kept || (x[u] == rintf(x[u]) && x[u] >= 0.0f));
                 }
                 hv[u] = m[u] >= 0;
                 col[u] = hv[u] ? __ldg(code + m[u]) : 0;
@@ -116,8 +127,8 @@ __global__ void __launch_bounds__(kExtractWarps * 32, 4) k_extract(DevChunk c, c
         double scale = 1.0;
         if (norm) {
             double total;
-            if (__all_sync(kFull, integral)) {
-                total = warp_sum(tsum);
+            if (__all_sync(kFull, integral && fsum < 16777216.0f)) {
+                total = warp_sum((double)fsum);  // integers: every order gives the in-order f64 sum
             } else {  // the reference's entry-order f64 sum
                 OrderedSum ts;
                 for_entries_by<4, false>(c, lo, hi, lookup, [&](int32_t m, float x) { ts.add(m != -1 ? (double)x : 0.0); });
@@ -208,14 +219,16 @@ template <int MODE>
 __global__ void __launch_bounds__(kDensifyCWarps * 32) k_densify_compact(
     const int64_t *__restrict__ indptr, int64_t cell0, int64_t n_cells, CompactHvg in, double target_sum, int log1p,
     DevScale t, const double *__restrict__ shift, int64_t d, int64_t d_pad, int64_t m_pad, void *tile,
-    double *__restrict__ colsum, int64_t *n_kept) {
+    double *__restrict__ colsum, long long *__restrict__ col_part, int64_t *n_kept) {
     using E = typename CElem<MODE>::T;
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr bool priv = MODE != 0;
     // column sums of the stored entries' scaled values in 32.32 fixed point
     // (native 64-bit integer shared atomics; exact, so the block's partial
-    // does not depend on the order of the adds); |s| >= 2^20 goes straight
-    // to the f64 global sum
+    // does not depend on the order of the adds); |s| >= 2^12 goes straight
+    // to the f64 global sum, so a tile's total (at most 2^13 cells) cannot
+    // overflow.  Each block writes its row of partials; k_colsum_reduce adds
+    // them up in block order.
     long long *s_col = reinterpret_cast<long long *>(smem);
     E *shift_row = reinterpret_cast<E *>(smem + (priv ? sizeof(double) * (size_t)round_up(d, 2) : 0));
     if (priv) {
@@ -269,7 +282,7 @@ __global__ void __launch_bounds__(kDensifyCWarps * 32) k_densify_compact(
                     row[sub] = h;
                     row_lo[sub] = l;
                 }
-                if (fabs(s) < 1048576.0)
+                if (fabs(s) < 4096.0)
                     atomicAdd(reinterpret_cast<unsigned long long *>(s_col + sub),
                               (unsigned long long)__double2ll_rn(s * 4294967296.0));
                 else
@@ -280,9 +293,21 @@ __global__ void __launch_bounds__(kDensifyCWarps * 32) k_densify_compact(
     if (lane == 0 && kept_count) atomicAdd(reinterpret_cast<unsigned long long *>(n_kept), (unsigned long long)kept_count);
     if (priv) {
         __syncthreads();
-        for (int64_t j = threadIdx.x; j < d; j += blockDim.x)
-            if (s_col[j] != 0) atomicAdd(colsum + j, (double)s_col[j] * 0x1.0p-32);
+        for (int64_t j = threadIdx.x; j < d; j += blockDim.x) col_part[(int64_t)blockIdx.x * d + j] = s_col[j];
     }
+}
+
+// colsum[j] += (sum over blocks of part[b][j]) 2^-32: an exact integer sum,
+// one warp per column (lanes over blocks).
+__global__ void k_colsum_reduce(const long long *__restrict__ part, int nb, int64_t d, double *__restrict__ colsum) {
+    const int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (j >= d) return;
+    long long s = 0;
+    for (int b = lane; b < nb; b += 32) s += part[(int64_t)b * d + j];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0 && s != 0) colsum[j] += (double)s * 0x1.0p-32;
 }
 
 template <int MODE>
@@ -296,12 +321,18 @@ static int densify_compact_t(const int64_t *indptr, int64_t cell0, int64_t n, co
     int per_sm = 0;
     CREST_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_densify_compact<MODE>,
                                                                  kDensifyCWarps * 32, smem));
-    // at most two blocks per SM: each block flushes its column sums once
-    const int64_t blocks =
-        std::min<int64_t>(ceil_div(m_pad, kDensifyCWarps), (int64_t)device_sms() * std::min(std::max(per_sm, 1), 2));
+    // at most two blocks per SM (the rows of the column-sum partials)
+    const int64_t blocks = std::min<int64_t>(ceil_div(m_pad, kDensifyCWarps),
+                                             std::min<int64_t>(w.colsum_rows, (int64_t)device_sms() * std::max(per_sm, 1)));
     k_densify_compact<MODE><<<(unsigned)blocks, kDensifyCWarps * 32, smem, st>>>(
-        indptr, cell0, n, in, target_sum, log1p, t, shift, w.d, w.d_pad, m_pad, w.tile, w.colsum_chunk, w.n_kept);
+        indptr, cell0, n, in, target_sum, log1p, t, shift, w.d, w.d_pad, m_pad, w.tile, w.colsum_chunk,
+        w.colsum_part, w.n_kept);
     CREST_CUDA_TRY(cudaGetLastError());
+    if (MODE != 0 && w.d > 0) {
+        k_colsum_reduce<<<(unsigned)ceil_div(w.d * 32, 256), 256, 0, st>>>(w.colsum_part, (int)blocks, w.d,
+                                                                          w.colsum_chunk);
+        CREST_CUDA_TRY(cudaGetLastError());
+    }
     return CREST_OK;
 }
 

@@ -228,21 +228,31 @@ __global__ void k_gemm_reduce(Gemm g, int ksplit, const double *__restrict__ ws)
 // subspace iteration): FP64 tensor-core MMAs (m8n8k4).
 //
 // CTA tile 64 x BN (BN = 16 NF), eight warps as 4 (M) x 2 (N), each warp
-// 16 x 8 NF outputs = 2 x NF fragments of 8 x 8.  K in steps of 16 through a
-// three-stage cp.async ring; shared-memory rows are padded so that each
-// half-warp's 8-byte fragment loads fall in 16 distinct 8-byte slots (row
-// strides of 68 and 20 doubles are 4 mod 16; op(A) = A^T is staged [m][k]
-// like B).  K is split over gridDim.z (about
-// two CTAs per SM); each slice writes its partial tile to ws, and the last
-// slice to finish (a per-tile arrival counter) sums all slices in slice order
-// and applies the epilogue, so results do not depend on scheduling.
+// 16 x 8 NF outputs = 2 x NF fragments of 8 x 8.  K in steps of 16 through an
+// ST-stage cp.async ring (more stages for narrow B, where the product streams
+// A at little arithmetic per byte); shared-memory rows are padded so that
+// each half-warp's 8-byte fragment loads fall in 16 distinct 8-byte slots
+// (row strides of 68 and 20 doubles are 4 mod 16; op(A) = A^T is staged
+// [m][k] like B).  K is split over gridDim.z = the cluster's z extent: every
+// slice leaves its partial tile in its own shared memory, and after a cluster
+// barrier slice r sums rows [64 r / ks, 64 (r + 1) / ks) of all slices'
+// partials in slice order (distributed shared memory), so results do not
+// depend on scheduling.
 namespace dm {
-constexpr int kBM = 64, kBK = 16, kStages = 3, kThreads = 256;
+constexpr int kBM = 64, kBK = 16, kThreads = 256;
 constexpr int kAS = kBM + 4;  // A stage: [k][m], m stride 68
 constexpr int kBS = kBK + 4;  // B stage: [n][k], k stride 20
-constexpr int kAStage = kBM * kBS > kBK * kAS ? kBM * kBS : kBK * kAS, kBStage = 64 * kBS;
-constexpr size_t kSmem = sizeof(double) * (size_t)kStages * (kAStage + kBStage);
-constexpr int kMaxTiles = 1024;
+constexpr int kAStage = kBM * kBS > kBK * kAS ? kBM * kBS : kBK * kAS;
+constexpr int kMaxSplit = 16;
+
+template <int NF>
+struct Cfg {
+    static constexpr int BN = 16 * NF;
+    static constexpr int ST = NF == 1 ? 6 : NF == 2 ? 4 : 3;
+    static constexpr int BStage = BN * kBS;
+    static constexpr size_t smem = sizeof(double) * (size_t)ST * (kAStage + BStage);
+    static_assert((size_t)ST * (kAStage + BStage) >= (size_t)kBM * BN, "partial tile must fit the ring");
+};
 
 __device__ __forceinline__ void cp16(void *smem, const void *gmem, bool ok) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -259,21 +269,30 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
                  : "+d"(c[0]), "+d"(c[1])
                  : "d"(a), "d"(b));
 }
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// generic address of the same shared-memory location in cluster CTA `rank`
+__device__ __forceinline__ const double *cluster_ptr(const double *p, unsigned rank) {
+    uint64_t r;
+    asm volatile("mapa.u64 %0, %1, %2;" : "=l"(r) : "l"(reinterpret_cast<uint64_t>(p)), "r"(rank));
+    return reinterpret_cast<const double *>(r);
+}
 
 template <int NF, bool TA>
-__global__ void __launch_bounds__(kThreads, 2) k_gemm_dmma(Gemm g, int kchunk, double *__restrict__ ws,
-                                                           int *__restrict__ cnt) {
-    constexpr int BN = 16 * NF;
+__global__ void __launch_bounds__(kThreads, 2) k_gemm_dmma(Gemm g, int kchunk) {
+    using C = Cfg<NF>;
+    constexpr int BN = C::BN, ST = C::ST;
     extern __shared__ __align__(16) double sm[];
-    double *As = sm, *Bs = sm + kStages * kAStage;
+    double *As = sm, *Bs = sm + ST * kAStage;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp & 3, wn = warp >> 2;
     const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN;
     const int kb = blockIdx.z * kchunk, ke = min(g.K, kb + kchunk);
-    const int ntiles = (ke - kb + kBK - 1) / kBK;
+    const int ntiles = ke > kb ? (ke - kb + kBK - 1) / kBK : 0;
 
     auto load = [&](int t, int stage) {
         const int k0 = kb + t * kBK;
-        double *as = As + stage * kAStage, *bs = Bs + stage * kBStage;
+        double *as = As + stage * kAStage, *bs = Bs + stage * C::BStage;
         // A: 16 k x 64 m = 512 chunks of two m ([k][m]), or of two k for A^T ([m][k])
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
@@ -306,18 +325,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_gemm_dmma(Gemm g, int kchunk, d
         for (int j = 0; j < NF; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
 #pragma unroll
-    for (int s = 0; s < kStages - 1; ++s) {
+    for (int s = 0; s < ST - 1; ++s) {
         if (s < ntiles) load(s, s);
         cp_commit();
     }
     const int ar = lane >> 2, ac = lane & 3;  // fragment row / column of this lane
     for (int t = 0; t < ntiles; ++t) {
-        cp_wait<kStages - 2>();
+        cp_wait<ST - 2>();
         __syncthreads();
-        if (t + kStages - 1 < ntiles) load(t + kStages - 1, (t + kStages - 1) % kStages);
+        if (t + ST - 1 < ntiles) load(t + ST - 1, (t + ST - 1) % ST);
         cp_commit();
-        const double *as = As + (t % kStages) * kAStage + (TA ? (wm * 16 + ar) * kBS + ac : wm * 16 + ar + ac * kAS);
-        const double *bs = Bs + (t % kStages) * kBStage + (wn * 8 * NF + ar) * kBS + ac;
+        const double *as =
+            As + (t % ST) * kAStage + (TA ? (wm * 16 + ar) * kBS + ac : wm * 16 + ar + ac * kAS);
+        const double *bs = Bs + (t % ST) * C::BStage + (wn * 8 * NF + ar) * kBS + ac;
 #pragma unroll
         for (int k4 = 0; k4 < kBK; k4 += 4) {
             double a[2], b[NF];
@@ -333,56 +353,53 @@ __global__ void __launch_bounds__(kThreads, 2) k_gemm_dmma(Gemm g, int kchunk, d
     }
     cp_wait<0>();
 
-    constexpr int R = 4 * NF;  // partial values per thread
-    const int tile = blockIdx.x + gridDim.x * blockIdx.y;
-    if (gridDim.z > 1) {
-        double *part = ws + ((int64_t)tile * gridDim.z + blockIdx.z) * R * kThreads + tid;
+    auto out = [&](int m, int n, double v) {
+        if (m >= g.M || n >= g.N) return;
+        const int64_t o = m + (int64_t)n * g.ldo;
+        double r = g.alpha * v;
+        if (g.X) r += g.beta * g.X[o];
+        if (g.Y) r += g.gamma * g.Y[o];
+        g.O[o] = r;
+    };
+    const int ks = (int)gridDim.z;
+    if (ks == 1) {
 #pragma unroll
         for (int i = 0; i < 2; ++i)
 #pragma unroll
             for (int j = 0; j < NF; ++j)
 #pragma unroll
-                for (int h = 0; h < 2; ++h) __stcg(part + ((i * NF + j) * 2 + h) * kThreads, acc[i][j][h]);
-        __threadfence();
-        __syncthreads();
-        __shared__ int last;
-        if (tid == 0) last = atomicAdd(cnt + tile, 1) == (int)gridDim.z - 1;
-        __syncthreads();
-        if (!last) return;
-        __threadfence();
-        const double *base = ws + (int64_t)tile * gridDim.z * R * kThreads + tid;
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-            for (int j = 0; j < NF; ++j)
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    double s = 0.0;
-                    for (int z = 0; z < (int)gridDim.z; ++z)
-                        s += __ldcg(base + ((int64_t)z * R + (i * NF + j) * 2 + h) * kThreads);
-                    acc[i][j][h] = s;
-                }
-        if (tid == 0) cnt[tile] = 0;  // ready for the next product
+                for (int h = 0; h < 2; ++h)
+                    out(m0 + wm * 16 + i * 8 + ar, n0 + wn * 8 * NF + j * 8 + ac * 2 + h, acc[i][j][h]);
+        return;
     }
+    // partial tile [m][n] in this CTA's ring, then the cluster-wide row split
+    __syncthreads();
+    double *part = sm;
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
         for (int j = 0; j < NF; ++j)
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int m = m0 + wm * 16 + i * 8 + ar, n = n0 + wn * 8 * NF + j * 8 + ac * 2 + h;
-                if (m >= g.M || n >= g.N) continue;
-                const int64_t o = m + (int64_t)n * g.ldo;
-                double v = g.alpha * acc[i][j][h];
-                if (g.X) v += g.beta * g.X[o];
-                if (g.Y) v += g.gamma * g.Y[o];
-                g.O[o] = v;
-            }
+            for (int h = 0; h < 2; ++h)
+                part[(wm * 16 + i * 8 + ar) * BN + wn * 8 * NF + j * 8 + ac * 2 + h] = acc[i][j][h];
+    cluster_sync_all();
+    const int r = (int)blockIdx.z, rows = kBM / ks, e0 = r * rows * BN, e1 = e0 + rows * BN;
+    const double *src[kMaxSplit];
+#pragma unroll
+    for (int z = 0; z < kMaxSplit; ++z) src[z] = z < ks ? cluster_ptr(part, (unsigned)z) : part;
+    for (int e = e0 + tid; e < e1; e += kThreads) {
+        double v = 0.0;
+#pragma unroll
+        for (int z = 0; z < kMaxSplit; ++z)
+            if (z < ks) v += src[z][e];
+        out(m0 + e / BN, n0 + e % BN, v);
+    }
+    cluster_sync_all();  // no CTA leaves while another reads its partial
 }
 }  // namespace dm
 
 struct GemmWs {
-    DevBuf ws, dws, cnt;
+    DevBuf ws;
 };
 
 static bool dmma_enabled() {  // CREST_EIG_DMMA=0: CUDA-core kernel for every product
@@ -399,37 +416,53 @@ static bool dmma_fits(const Gemm &g) {
            !(g.ldb & 1) && (g.tA || !(g.M & 1)) && al(g.A) && al(g.B);
 }
 
-template <int NF>
-static int launch_dmma(const Gemm &g, dim3 grid, int kchunk, double *ws, int *cnt, cudaStream_t st) {
-    if (g.tA) {
-        CREST_TRY(ensure_smem_attr((const void *)dm::k_gemm_dmma<NF, true>, dm::kSmem));
-        dm::k_gemm_dmma<NF, true><<<grid, dm::kThreads, dm::kSmem, st>>>(g, kchunk, ws, cnt);
-    } else {
-        CREST_TRY(ensure_smem_attr((const void *)dm::k_gemm_dmma<NF, false>, dm::kSmem));
-        dm::k_gemm_dmma<NF, false><<<grid, dm::kThreads, dm::kSmem, st>>>(g, kchunk, ws, cnt);
+template <int NF, bool TA>
+static int launch_dmma(const Gemm &g, int mt, int nt, int ks, int kchunk, cudaStream_t st) {
+    const void *fn = (const void *)dm::k_gemm_dmma<NF, TA>;
+    CREST_TRY(ensure_smem_attr(fn, dm::Cfg<NF>::smem));
+    static bool nonportable = [fn] {
+        const bool ok = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
+        (void)cudaGetLastError();
+        return ok;
+    }();
+    if (!nonportable && ks > 8) ks = 8;
+    auto launch = [&](int z) {
+        const int kc = z > 1 ? (int)round_up(ceil_div(g.K, z), dm::kBK) : kchunk;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(mt, nt, z);
+        cfg.blockDim = dim3(dm::kThreads);
+        cfg.dynamicSmemBytes = dm::Cfg<NF>::smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 1;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = z;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        return cudaLaunchKernelEx(&cfg, dm::k_gemm_dmma<NF, TA>, g, kc);
+    };
+    cudaError_t e = launch(ks);
+    if (e != cudaSuccess && ks > 8) {  // a 16-CTA cluster that cannot be placed: 8 slices
+        (void)cudaGetLastError();
+        e = launch(8);
     }
-    CREST_CUDA_TRY(cudaGetLastError());
+    CREST_CUDA_TRY(e);
     return CREST_OK;
 }
 
-static int gemm_dmma(const Gemm &g, GemmWs &w, cudaStream_t st) {
+// K split: about two CTAs per SM, a power of two (the cluster extent) up to
+// 16, slices of at least 64.
+static int gemm_dmma(const Gemm &g, GemmWs &, cudaStream_t st) {
     const int nf = g.N <= 16 ? 1 : g.N <= 32 ? 2 : 4;
     const int mt = (int)ceil_div(g.M, dm::kBM), nt = (int)ceil_div(g.N, 16 * nf);
-    int ks = std::max(1, std::min((2 * device_sms()) / (mt * nt), g.K / (4 * dm::kBK)));
-    const int kchunk = (int)round_up(ceil_div(g.K, ks), dm::kBK);
-    ks = (int)ceil_div(g.K, kchunk);
-    CREST_REQUIRE(mt * nt <= dm::kMaxTiles, CREST_EINVAL, "GEMM too large for the tile counters");
-    if (!w.cnt.ptr) {
-        CREST_TRY(w.cnt.ensure(sizeof(int) * dm::kMaxTiles));
-        CREST_CUDA_TRY(cudaMemsetAsync(w.cnt.ptr, 0, sizeof(int) * dm::kMaxTiles, st));
-    }
-    if (ks > 1) CREST_TRY(w.dws.ensure(sizeof(double) * (size_t)mt * nt * ks * 4 * nf * dm::kThreads));
-    const dim3 grid(mt, nt, ks);
-    double *ws = w.dws.as<double>();
-    int *cnt = w.cnt.as<int>();
-    if (nf == 1) return launch_dmma<1>(g, grid, kchunk, ws, cnt, st);
-    if (nf == 2) return launch_dmma<2>(g, grid, kchunk, ws, cnt, st);
-    return launch_dmma<4>(g, grid, kchunk, ws, cnt, st);
+    const int want = std::max(1, std::min((2 * device_sms()) / (mt * nt), g.K / (4 * dm::kBK)));
+    int ks = 1;
+    while (ks * 2 <= want && ks * 2 <= dm::kMaxSplit) ks *= 2;
+    const int kchunk = ks > 1 ? (int)round_up(ceil_div(g.K, ks), dm::kBK) : g.K;
+    if (nf == 1) return g.tA ? launch_dmma<1, true>(g, mt, nt, ks, kchunk, st) : launch_dmma<1, false>(g, mt, nt, ks, kchunk, st);
+    if (nf == 2) return g.tA ? launch_dmma<2, true>(g, mt, nt, ks, kchunk, st) : launch_dmma<2, false>(g, mt, nt, ks, kchunk, st);
+    return g.tA ? launch_dmma<4, true>(g, mt, nt, ks, kchunk, st) : launch_dmma<4, false>(g, mt, nt, ks, kchunk, st);
 }
 
 int gemm(const Gemm &g, GemmWs &w, cudaStream_t st) {
@@ -606,7 +639,8 @@ static int jacobi_threads() {
     return v < 64 ? 64 : (v > 512 ? 512 : v);
 }
 
-int jacobi(const double *A, int n_in, double *Vwork, double *V, double *vals, int *sweeps, cudaStream_t st) {
+int jacobi(const double *A, int n_in, double *Vwork, double *V, double *vals, int *sweeps, cudaStream_t st,
+           int max_sweeps = 40) {
     const int n = n_in + (n_in & 1);
     CREST_REQUIRE(n <= kJacobiMax, CREST_EINVAL, "Jacobi size %d exceeds %d", n, kJacobiMax);
     prof::Scope ps("eig_jacobi", st);
@@ -614,11 +648,11 @@ int jacobi(const double *A, int n_in, double *Vwork, double *V, double *vals, in
     if (n <= kJacobiSmemV) {
         const size_t smem = sizeof(double) * ((size_t)n * (n + 1) + (size_t)n * n);
         CREST_TRY(ensure_smem_attr((const void *)k_jacobi<true>, (size_t)smem));
-        k_jacobi<true><<<1, nt, smem, st>>>(A, n_in, n, nullptr, V, vals, 40, sweeps);
+        k_jacobi<true><<<1, nt, smem, st>>>(A, n_in, n, nullptr, V, vals, max_sweeps, sweeps);
     } else {
         const size_t smem = sizeof(double) * (size_t)n * (size_t)(n + 1);
         CREST_TRY(ensure_smem_attr((const void *)k_jacobi<false>, (size_t)smem));
-        k_jacobi<false><<<1, nt, smem, st>>>(A, n_in, n, Vwork, V, vals, 40, sweeps);
+        k_jacobi<false><<<1, nt, smem, st>>>(A, n_in, n, Vwork, V, vals, max_sweeps, sweeps);
     }
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
@@ -775,6 +809,69 @@ __global__ void __launch_bounds__(1024) k_cgs2(double *Q, int64_t d, int j0, int
 // Rinv = I, leaving Y unchanged) when a column is zero or a pivot is not
 // positive.
 constexpr int kCholNb = 16;
+
+// The same factor for p <= 64 with one barrier per step: the matrix stays
+// in shared memory, every thread reads the step's pivot itself, and the
+// trailing update uses the unscaled column (A_ij -= A_ik A_jk / A_kk); L^-1
+// follows by right-looking substitution on the identity, rows scaled at the
+// end.  Rinv and the failure flag have the meaning of k_chol_inv's.
+constexpr int kCholSmall = 64;
+
+__global__ void __launch_bounds__(256) k_chol_inv_small(const double *__restrict__ B, int p, double shift_coef,
+                                                        double *__restrict__ Rinv, int *fail) {
+    extern __shared__ double chol_smem[];
+    auto A = reinterpret_cast<double(*)[kCholSmall + 1]>(chol_smem);  // [i][j], lower triangle
+    auto R = A + kCholSmall;                                          // right-hand sides -> L^-1, [i][c]
+    __shared__ double dsc[kCholSmall], rl[kCholSmall];
+    __shared__ int bad;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (tid == 0) bad = 0;
+    __syncthreads();
+    for (int i = tid; i < p; i += nt) {
+        const double b = B[i + (int64_t)i * p];
+        if (!(b > 0.0)) bad = 1;
+        dsc[i] = b > 0.0 ? 1.0 / sqrt(b) : 1.0;
+    }
+    __syncthreads();
+    const double shift = shift_coef * (double)p;
+    for (int w = tid; w < p * p; w += nt) {
+        const int i = w % p, j = w / p;
+        A[i][j] = (i == j) ? 1.0 + shift : B[w] * dsc[i] * dsc[j];
+        R[i][j] = (i == j) ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    for (int k = 0; k < p; ++k) {
+        const double akk = A[k][k];
+        const double piv = akk > 0.0 ? akk : 1.0;
+        const double rp = 1.0 / piv;
+        const int m = p - k - 1;
+        for (int w = tid; w < m * m; w += nt) {
+            const int i = k + 1 + w % m, j = k + 1 + w / m;
+            if (i >= j) A[i][j] -= A[i][k] * A[j][k] * rp;
+        }
+        if (tid == 0) {
+            if (!(akk > 0.0)) bad = 1;
+            rl[k] = 1.0 / sqrt(piv);
+        }
+        __syncthreads();
+    }
+    // L X = I with L_ik = A_ik rl_k: row i of X is R_i rl_i once rows < i are applied
+    for (int i = 0; i < p; ++i) {
+        const int m = p - i - 1, n = i + 1;
+        const double ri = rl[i];
+        for (int w = tid; w < m * n; w += nt) {
+            const int t = i + 1 + w % m, c = w / m;
+            R[t][c] -= (A[t][i] * ri) * (R[i][c] * ri);
+        }
+        __syncthreads();
+    }
+    // Rinv = D (L^-1)^T, or the identity (Y left as it is) when the factor failed
+    for (int w = tid; w < p * p; w += nt) {
+        const int r = w % p, c = w / p;
+        Rinv[w] = bad ? (r == c ? 1.0 : 0.0) : (r <= c ? dsc[r] * R[c][r] * rl[c] : 0.0);
+    }
+    if (tid == 0 && bad) *fail = 1;
+}
 
 __global__ void __launch_bounds__(512) k_chol_inv(const double *__restrict__ B, int p, double shift_coef,
                                                   double *__restrict__ Rinv, int *fail) {
@@ -985,16 +1082,21 @@ __global__ void __launch_bounds__(1024) k_lanczos_step(double *V, int64_t d, int
     }
 }
 
-// All L Lanczos steps in one cooperative launch (one CTA per SM, rows of C
-// and of the basis split evenly over the CTAs).  Per step, three grid
-// barriers:
-//   1. w' = C v_j / beta_{j-1} on this CTA's rows (v_j = w / beta_{j-1}
-//      is normalised on the fly; row i of C is its column i), and the
-//      partial dots of those rows with v_0..v_j;
-//   2. h = the sum of the partials in CTA order; w' -= V h on this CTA's
-//      rows, and the partials of the second Gram-Schmidt pass;
-//   3. the same subtraction again, and the partial squared norm.
-// alpha_j is the first-pass coefficient of v_j.  All sums run in a fixed
+// All L Lanczos steps in one cooperative launch (one CTA per SM).  CTA b
+// owns rows [r0, r1) of C and of the basis: it keeps those rows of C in
+// shared memory as FP32 (the run only brackets the spectrum: FP32 products
+// move the extreme Ritz values by ~1e-7 relative, far inside the guard the
+// filter interval keeps) and its slice of the basis in FP64, so only the
+// current vector crosses the grid.  Per step, three grid barriers:
+//   1. w' = C v_j / beta_{j-1} on the owned rows (v_j = w / beta_{j-1} is
+//      normalised on the fly), and the partial dots of those rows with
+//      v_0..v_j;
+//   2. h = the sum of the partials over CTAs (a fixed shuffle tree);
+//      w' -= V h on the owned rows, and the second Gram-Schmidt pass's
+//      partials;
+//   3. the same subtraction again, w' published for the next product, and
+//      the partial squared norm.
+// alpha_j is the first-pass coefficient of v_j.  Every sum runs in a fixed
 // order, so the run is deterministic.  Each barrier wait is bounded (about
 // one second of %globaltimer); on expiry the CTA raises *err and every later
 // barrier is skipped, so the launch always ends.
@@ -1004,26 +1106,27 @@ __device__ __forceinline__ unsigned long long gtimer() {
     return t;
 }
 
-__device__ void grid_barrier(unsigned *bar, unsigned nblk, int *err) {
+// Grid barrier on a counter that only grows (zeroed before the launch):
+// barrier number `phase` is passed once it reaches phase x nblk, so every CTA
+// arrives with one atomic and leaves as soon as it reads the total -- no
+// second round trip through a generation word.
+__device__ void grid_barrier(unsigned *count, unsigned &phase, unsigned nblk, int *err) {
     __syncthreads();
+    ++phase;
     if (threadIdx.x == 0) {
-        volatile unsigned *gen = bar + 1;
         volatile int *e = err;
         if (!*e) {
-            const unsigned g = *gen;
+            const unsigned target = phase * nblk;
             __threadfence();
-            if (atomicAdd(bar, 1u) == nblk - 1) {
-                atomicExch(bar, 0u);
-                __threadfence();
-                atomicAdd(bar + 1, 1u);
-            } else {
-                const unsigned long long t0 = gtimer();
-                while (*gen == g) {
-                    if (*e || gtimer() - t0 > 1000000000ull) {
-                        atomicExch(err, 1);
-                        break;
-                    }
-                    __nanosleep(64);
+            atomicAdd(count, 1u);
+            const unsigned long long t0 = gtimer();
+            for (;;) {
+                unsigned v;
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+                if (v >= target) break;
+                if (*e || gtimer() - t0 > 1000000000ull) {
+                    atomicExch(err, 1);
+                    break;
                 }
             }
         }
@@ -1036,84 +1139,131 @@ struct LanczosArgs {
     const double *C;
     int64_t d;
     int L;
-    double *Z;     // d x (kLanczos + 1), column 0 = the normalised start vector
-    double *w[2];  // d each
+    int rows;      // rows per CTA (the last CTAs may own fewer)
+    const double *z0;  // the normalised start vector
+    double *w;     // d: the current (unnormalised) vector, published each step
     double *part;  // gridDim.x x 3 x (kLanczos + 1)
     double *ab;    // alpha [0, kLanczos), beta [kLanczos, 2 kLanczos)
     unsigned *bar;
     int *err;
 };
 
+constexpr int kLzP = kLanczos + 1;
+
+size_t lanczos_smem(int64_t d, int rows) {
+    return sizeof(float) * (size_t)rows * d + sizeof(double) * ((size_t)d + (size_t)kLzP * rows + rows);
+}
+
 __global__ void __launch_bounds__(512) k_lanczos(LanczosArgs a) {
-    constexpr int P = kLanczos + 1;
-    __shared__ double coef[P];
+    extern __shared__ __align__(16) unsigned char lz_smem[];
+    __shared__ double coef[kLzP], red[16];
     __shared__ double scal;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
     const unsigned nb = gridDim.x, b = blockIdx.x;
-    const int64_t d = a.d, r0 = d * b / nb, r1 = d * (b + 1) / nb;
-    double *part = a.part + (size_t)b * 3 * P;
-    // the start vector plays the role of w with beta = 1
-    for (int64_t r = r0 + tid; r < r1; r += nt) a.w[1][r] = a.Z[r];
-    if (tid == 0) scal = 1.0;
-    grid_barrier(a.bar, nb, a.err);
+    const int64_t d = a.d;
+    const int64_t r0 = min(d, (int64_t)b * a.rows), r1 = min(d, r0 + a.rows);
+    const int R = (int)(r1 - r0);
+    double *wv = reinterpret_cast<double *>(lz_smem);  // d: the vector being multiplied
+    double *zs = wv + d;                               // kLzP x rows: owned slice of the basis
+    double *wl = zs + (size_t)kLzP * a.rows;           // rows: owned slice of w'
+    float *cs = reinterpret_cast<float *>(wl + a.rows);  // rows x d: owned rows of C
+    for (int64_t e = tid; e < (int64_t)R * d; e += nt) cs[e] = (float)a.C[r0 * d + e];
+    for (int64_t e = tid; e < d; e += nt) wv[e] = a.z0[e];
+    if (tid == 0) scal = 1.0;  // the start vector plays the role of w with beta = 1
+    double *part = a.part + (size_t)b * 3 * kLzP;
+    unsigned phase = 0;
+    __syncthreads();
     for (int j = 0; j < a.L; ++j) {
-        const double *win = a.w[(j + 1) & 1];
-        double *wout = a.w[j & 1];
-        const double inv = 1.0 / scal;  // 1 / beta_{j-1}
-        double *vj = a.Z + (int64_t)j * d;
-        for (int64_t r = r0 + tid; r < r1; r += nt) vj[r] = win[r] * inv;
-        for (int64_t r = r0 + wid; r < r1; r += nw) {  // row r of C = column r
-            const double *col = a.C + r * d;
-            double t = 0.0;
-            for (int64_t i = lane; i < d; i += 32) t += col[i] * win[i];
+        if (j > 0)
+            for (int64_t e = tid; e < d; e += nt) wv[e] = __ldcg(a.w + e);
+        __syncthreads();
+        const double inv = 1.0 / scal;
+        for (int rr = tid; rr < R; rr += nt) zs[j * a.rows + rr] = wv[r0 + rr] * inv;
+        for (int rr = wid; rr < R; rr += nw) {
+            const float *row = cs + (size_t)rr * d;
+            double t0 = 0.0, t1 = 0.0;
+            int64_t i = lane;
+            for (; i + 32 < d; i += 64) {
+                t0 += (double)row[i] * wv[i];
+                t1 += (double)row[i + 32] * wv[i + 32];
+            }
+            if (i < d) t0 += (double)row[i] * wv[i];
+            double t = t0 + t1;
             for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-            if (lane == 0) wout[r] = t * inv;
+            if (lane == 0) wl[rr] = t * inv;
         }
         __syncthreads();
         for (int pass = 0; pass < 3; ++pass) {
-            double *pp = part + pass * P;
-            if (pass < 2) {  // partial dots of this CTA's rows with v_0..v_j
+            double *pp = part + pass * kLzP;
+            if (pass < 2) {  // partial dots of the owned rows with v_0..v_j
                 for (int i = wid; i <= j; i += nw) {
-                    const double *zi = a.Z + (int64_t)i * d;
                     double t = 0.0;
-                    for (int64_t r = r0 + lane; r < r1; r += 32) t += zi[r] * wout[r];
+                    for (int rr = lane; rr < R; rr += 32) t += zs[i * a.rows + rr] * wl[rr];
                     for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
                     if (lane == 0) pp[i] = t;
                 }
             } else {
                 double t = 0.0;
-                for (int64_t r = r0 + tid; r < r1; r += nt) t += wout[r] * wout[r];
+                for (int rr = tid; rr < R; rr += nt) t += wl[rr] * wl[rr];
                 for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-                if (lane == 0) coef[wid] = t;
+                if (lane == 0) red[wid] = t;
                 __syncthreads();
                 if (tid == 0) {
-                    double s = 0.0;
-                    for (int i = 0; i < nw; ++i) s += coef[i];
-                    pp[0] = s;
+                    double s2 = 0.0;
+                    for (int i = 0; i < nw; ++i) s2 += red[i];
+                    pp[0] = s2;
                 }
             }
-            grid_barrier(a.bar, nb, a.err);
+            grid_barrier(a.bar, phase, nb, a.err);
             if (pass == 2) break;
-            for (int i = tid; i <= j; i += nt) {  // coefficients, summed in CTA order
-                double s = 0.0;
-                for (unsigned c = 0; c < nb; ++c) s += __ldcg(a.part + ((size_t)c * 3 + pass) * P + i);
-                coef[i] = s;
+            // coefficients: warp w sums those of i = w, w + 16, ... (lanes over
+            // CTAs, a fixed shuffle tree), all of its loads issued at once
+            {
+                constexpr int kI = (kLzP + 15) / 16, kC = 8;  // i per warp, CTAs per lane (<= 256 CTAs)
+                double v[kI][kC];
+#pragma unroll
+                for (int q = 0; q < kI; ++q)
+#pragma unroll
+                    for (int t = 0; t < kC; ++t) {
+                        const int i = wid + 16 * q;
+                        const unsigned c = lane + 32 * t;
+                        v[q][t] = (i <= j && c < nb) ? __ldcg(a.part + ((size_t)c * 3 + pass) * kLzP + i) : 0.0;
+                    }
+#pragma unroll
+                for (int q = 0; q < kI; ++q) {
+                    double s2 = 0.0;
+#pragma unroll
+                    for (int t = 0; t < kC; ++t) s2 += v[q][t];
+                    for (int o = 16; o; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+                    if (lane == 0 && wid + 16 * q <= j) coef[wid + 16 * q] = s2;
+                }
             }
             __syncthreads();
             if (pass == 0 && b == 0 && tid == 0) a.ab[j] = coef[j];
-            for (int64_t r = r0 + tid; r < r1; r += nt) {
-                double v = wout[r];
-                for (int i = 0; i <= j; ++i) v -= coef[i] * a.Z[(int64_t)i * d + r];
-                wout[r] = v;
+            for (int rr = tid; rr < R; rr += nt) {
+                double v = wl[rr];
+                for (int i = 0; i <= j; ++i) v -= coef[i] * zs[i * a.rows + rr];
+                wl[rr] = v;
+                if (pass == 1) a.w[r0 + rr] = v;  // published before the last barrier of the step
             }
             __syncthreads();
         }
-        if (tid == 0) {
-            double s = 0.0;
-            for (unsigned c = 0; c < nb; ++c) s += __ldcg(a.part + ((size_t)c * 3 + 2) * P);
-            const double beta = sqrt(s);
-            scal = beta > 0.0 ? beta : 1.0;
-            if (b == 0) a.ab[kLanczos + j] = beta;
+        if (wid == 0) {
+            double v[8];
+#pragma unroll
+            for (int t = 0; t < 8; ++t) {
+                const unsigned c = lane + 32 * t;
+                v[t] = c < nb ? __ldcg(a.part + ((size_t)c * 3 + 2) * kLzP) : 0.0;
+            }
+            double s2 = 0.0;
+#pragma unroll
+            for (int t = 0; t < 8; ++t) s2 += v[t];
+            for (int o = 16; o; o >>= 1) s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+            const double beta = sqrt(s2);
+            if (lane == 0) {
+                scal = beta > 0.0 ? beta : 1.0;
+                if (b == 0) a.ab[kLanczos + j] = beta;
+            }
         }
         __syncthreads();
     }
@@ -1140,21 +1290,28 @@ int lanczos_coop(EigWork &w, const double *C, int64_t d, int L, cudaStream_t st)
         return e && e[0] == '0';
     }();
     if (off) return CREST_ERUNTIME;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lanczos, 512, 0) != cudaSuccess || per_sm < 1) {
+    // at most 256 CTAs: each lane of the coefficient sums reads 8 CTAs' partials
+    const int nb = (int)std::min<int64_t>(std::min(device_sms(), 256), std::max<int64_t>(1, d / 4));
+    const int rows = (int)ceil_div(d, nb);
+    const size_t smem = lanczos_smem(d, rows);
+    if (smem > (size_t)kMaxSmem || ensure_smem_attr((const void *)k_lanczos, smem) != CREST_OK) {
         (void)cudaGetLastError();
         return CREST_ERUNTIME;
     }
-    const int nb = (int)std::min<int64_t>(device_sms(), std::max<int64_t>(1, d / 4));
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lanczos, 512, smem) != cudaSuccess || per_sm < 1) {
+        (void)cudaGetLastError();
+        return CREST_ERUNTIME;
+    }
     CREST_TRY(w.lw2.ensure(sizeof(double) * (size_t)d));
     CREST_TRY(w.lpart.ensure(sizeof(double) * (size_t)nb * 3 * (kLanczos + 1)));
     CREST_TRY(w.lbar.ensure(sizeof(unsigned) * 2));
     CREST_CUDA_TRY(cudaMemsetAsync(w.lbar.ptr, 0, sizeof(unsigned) * 2, st));
     CREST_CUDA_TRY(cudaMemsetAsync(w.fail.as<int>() + 3, 0, sizeof(int), st));
-    LanczosArgs a{C, d, L, w.lz.as<double>(), {w.lw.as<double>(), w.lw2.as<double>()}, w.lpart.as<double>(),
+    LanczosArgs a{C, d, L, rows, w.lz.as<double>(), w.lw2.as<double>(), w.lpart.as<double>(),
                   w.lab.as<double>(), w.lbar.as<unsigned>(), w.fail.as<int>() + 3};
     void *args[] = {&a};
-    if (cudaLaunchCooperativeKernel((const void *)k_lanczos, dim3(nb), dim3(512), args, 0, st) != cudaSuccess) {
+    if (cudaLaunchCooperativeKernel((const void *)k_lanczos, dim3(nb), dim3(512), args, smem, st) != cudaSuccess) {
         (void)cudaGetLastError();
         return CREST_ERUNTIME;
     }
@@ -1189,7 +1346,11 @@ int orthonormalise(EigWork &w, double *Y, int64_t d, int j0, int q, bool shifted
         const double shift_coef = (shifted && pass == 0) ? 11.0 * ((double)d * q + (double)q * (q + 1)) * 0x1.0p-53 : 0.0;
         {
             prof::Scope ps("eig_cholqr", st);
-            k_chol_inv<<<1, 512, csmem, st>>>(B, q, shift_coef, Rinv, fail);
+            constexpr size_t small_smem = sizeof(double) * 2 * kCholSmall * (kCholSmall + 1);
+            if (q <= kCholSmall && ensure_smem_attr((const void *)k_chol_inv_small, small_smem) == CREST_OK)
+                k_chol_inv_small<<<1, 256, small_smem, st>>>(B, q, shift_coef, Rinv, fail);
+            else
+                k_chol_inv<<<1, 512, csmem, st>>>(B, q, shift_coef, Rinv, fail);
         }
         CREST_CUDA_TRY(cudaGetLastError());
         CREST_TRY(gemm(Gemm{D, q, q, Ya, D, 0, Rinv, q, T, D, 1.0, nullptr, 0.0, nullptr, 0.0}, w.g, st));
@@ -1359,7 +1520,11 @@ int eig_topk(const double *G, const double *colsum, int64_t d, int64_t n, int64_
         CREST_TRY(gemm(Gemm{q, q, D, Va, D, 1, Wa, D, H, q, 1.0, nullptr, 0.0, nullptr, 0.0}, w.g, st));
         k_symmetrise<<<(unsigned)ceil_div(q * q, 256), 256, 0, st>>>(H, q);
         CREST_CUDA_TRY(cudaGetLastError());
-        CREST_TRY(jacobi(H, q, Y0, Q, jvals, nullptr, st));
+        // While the wanted residuals are far from converged the Ritz vectors
+        // only have to span the block (the filter acts on the subspace), so
+        // two sweeps stand in for the full diagonalisation; the Ritz values
+        // (diagonal of the partly rotated H) only set the filter interval.
+        CREST_TRY(jacobi(H, q, Y0, Q, jvals, nullptr, st, res_max > 1e-5 ? 2 : 40));
         k_rank<<<(unsigned)ceil_div(q, 128), 128, 0, st>>>(jvals, q, perm, sorted + locked);
         CREST_CUDA_TRY(cudaGetLastError());
         k_permute_cols<<<(unsigned)ceil_div(q * q, 256), 256, 0, st>>>(Q, H, q, perm, q);

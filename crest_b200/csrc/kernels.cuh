@@ -123,6 +123,8 @@ struct GramWork {
                             // be checked (unsorted, more HVG entries than the densify queue)
     double *gram_aux;       // [d x d] BF16X3: Gram of the second cell half of each tile (CTA-pair
                             // SYRK), zero between passes; folded by gram_aux_fold
+    long long *colsum_part;  // [colsum_rows x d] per-block column sums (32.32 fixed point)
+    int64_t colsum_rows;
 };
 
 size_t gram_tile_bytes(int precision, int64_t d_pad, int64_t m_cap);

@@ -181,9 +181,14 @@ typedef struct crest_pca crest_pca;
 
 /* A CSR count matrix (cells x genes): indptr i64[n_cells+1] (indptr[0] == 0),
  * indices u32[nnz], data f32[nnz], all in host memory.
- * residency CREST_MEM_DEVICE copies it to HBM once; CREST_MEM_HOST keeps it
- * in (ideally pinned) host memory and streams chunks of chunk_cells cells
- * through two device buffers on every pass. */
+ * residency CREST_MEM_DEVICE copies it to HBM once: the copy of indices /
+ * data runs asynchronously in chunks of 131,072 cells (from pinned memory it
+ * overlaps the first Gram pass, which consumes each chunk as it arrives), so
+ * indices and data must stay valid and unchanged until the first operation
+ * on the matrix has returned (or until crest_matrix_free); indptr is copied
+ * before this call returns.  CREST_MEM_HOST keeps it in (ideally pinned)
+ * host memory and streams chunks of chunk_cells cells through two device
+ * buffers on every pass. */
 int crest_matrix_create(crest_matrix **out, const int64_t *indptr, const uint32_t *indices,
                         const float *data, int64_t n_cells, int64_t n_genes, int32_t residency,
                         int64_t chunk_cells);
