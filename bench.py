@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-fused", action="store_true")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="only the timed bf16x3 steps (for profiler launch lists): no CPU baseline, no FP32 / FP64 "
+                         "legs, no memory-bound passes, no e2e")
     return ap.parse_args()
 
 
@@ -277,6 +280,8 @@ def run_reference(args):
 
 # ------------------------------------------------------------------ GPU arm
 def main_gpu(args):
+    if args.kernels_only:
+        args.no_cpu = args.no_fp32 = args.no_fused = True
     import torch
     import crest_b200 as cb
     from crest_b200 import _lib, tl
@@ -388,6 +393,12 @@ def main_gpu(args):
         extra["speedup_bf16x3_vs_fp32"] = r_32["ms"] / ms
         # the Gram phase is the only part that differs between the two forms
         extra["speedup_gram_bf16x3_vs_fp32"] = r_32["stats"]["gram_ms"] / stats["gram_ms"]
+    if args.kernels_only:
+        print(json.dumps({"metric": METRIC, "value": n_rows * ws / (ms / 1e3), "unit": UNIT, "n_gpus": ws,
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                          "kernels_ms_per_step": {kk: vv[1] / args.steps for kk, vv in table.items()},
+                          "note": "kernels-only run"}))
+        return 0
     # accuracy of the product and plain forms against the FP64 Gram of the same run
     r_64 = timed("fp64", 1, 0, keep_scores=want_parity)
     extra["max_principal_angle_deg_vs_fp64"] = subspace_angle_deg(r_bf["loadings"], r_64["loadings"])

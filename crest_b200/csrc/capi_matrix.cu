@@ -33,6 +33,7 @@ struct crest_matrix {
     // already waits for every chunk.
     std::vector<int64_t> up_end;
     std::vector<cudaEvent_t> up_ev;
+    size_t up_issued = 0;  // chunks whose copies have been queued (in order)
     bool up_waited = true;
     crest::DevBuf buf_idx[2], buf_val[2];
     cudaEvent_t ev_ready[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
@@ -80,9 +81,31 @@ namespace {
 
 constexpr int64_t kUploadCells = 131072;  // cells per upload chunk (a multiple of the Gram tile)
 
+// Queue the copies of upload chunks [up_issued, upto).  Chunks are queued a
+// little ahead of their use rather than all at matrix creation: copies from
+// pageable memory made later (the maps of a pass) then do not wait behind
+// the whole matrix on the copy engine.
+int issue_uploads(crest_matrix *m, size_t upto) {
+    upto = std::min(upto, m->up_ev.size());
+    for (; m->up_issued < upto; ++m->up_issued) {
+        const size_t u = m->up_issued;
+        const int64_t c0 = u ? m->up_end[u - 1] : 0, c1 = m->up_end[u];
+        const int64_t e0 = m->h_indptr[c0], e1 = m->h_indptr[c1];
+        if (e1 > e0) {
+            CREST_CUDA_TRY(cudaMemcpyAsync(m->d_indices.as<uint32_t>() + e0, m->h_indices + e0, 4 * (size_t)(e1 - e0),
+                                           cudaMemcpyHostToDevice, m->copy));
+            CREST_CUDA_TRY(cudaMemcpyAsync(m->d_data.as<float>() + e0, m->h_data + e0, 4 * (size_t)(e1 - e0),
+                                           cudaMemcpyHostToDevice, m->copy));
+        }
+        CREST_CUDA_TRY(cudaEventRecord(m->up_ev[u], m->copy));
+    }
+    return CREST_OK;
+}
+
 // The compute stream waits for every upload chunk (once per matrix).
 int wait_upload(crest_matrix *m) {
     if (m->up_waited || m->up_ev.empty()) return CREST_OK;
+    CREST_TRY(issue_uploads(m, m->up_ev.size()));
     CREST_CUDA_TRY(cudaStreamWaitEvent(m->compute, m->up_ev.back(), 0));
     m->up_waited = true;
     return CREST_OK;
@@ -422,29 +445,21 @@ int crest_matrix_create(crest_matrix **out, const int64_t *indptr, const uint32_
         rc = m->d_indices.ensure(4 * (size_t)std::max<int64_t>(nnz, 1));
         if (!rc) rc = m->d_data.ensure(4 * (size_t)std::max<int64_t>(nnz, 1));
         if (rc) return fail(rc);
+        m->h_indices = indices;
+        m->h_data = data;
         for (int64_t c0 = 0; c0 < n_cells || (c0 == 0 && n_cells == 0); c0 += kUploadCells) {
-            const int64_t c1 = std::min(n_cells, c0 + kUploadCells), e0 = indptr[c0], e1 = indptr[c1];
-            if (e1 > e0) {
-                if (cudaMemcpyAsync(m->d_indices.as<uint32_t>() + e0, indices + e0, 4 * (size_t)(e1 - e0),
-                                    cudaMemcpyHostToDevice, m->copy) != cudaSuccess ||
-                    cudaMemcpyAsync(m->d_data.as<float>() + e0, data + e0, 4 * (size_t)(e1 - e0),
-                                    cudaMemcpyHostToDevice, m->copy) != cudaSuccess) {
-                    set_error("matrix upload failed: %s", cudaGetErrorString(cudaGetLastError()));
-                    return fail(CREST_ECUDA);
-                }
-            }
             cudaEvent_t ev = nullptr;
-            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess ||
-                cudaEventRecord(ev, m->copy) != cudaSuccess) {
-                if (ev) cudaEventDestroy(ev);
+            if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
                 set_error("matrix upload failed: %s", cudaGetErrorString(cudaGetLastError()));
                 return fail(CREST_ECUDA);
             }
             m->up_ev.push_back(ev);
-            m->up_end.push_back(c1);
+            m->up_end.push_back(std::min(n_cells, c0 + kUploadCells));
             if (n_cells == 0) break;
         }
         m->up_waited = false;
+        rc = issue_uploads(m, 1);  // the first chunk now, the rest as passes consume them
+        if (rc) return fail(rc);
     } else {
         m->h_indices = indices;
         m->h_data = data;
@@ -710,7 +725,10 @@ int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
         int64_t u0 = 0;
         for (size_t u = 0; u < m->up_end.size() && u0 < m->n_cells; ++u) {
             const int64_t u1 = m->up_end[u];
-            if (!m->up_waited) CREST_CUDA_TRY(cudaStreamWaitEvent(st, m->up_ev[u], 0));
+            if (!m->up_waited) {
+                CREST_TRY(issue_uploads(m, u + 2));  // keep the next chunk's copy queued
+                CREST_CUDA_TRY(cudaStreamWaitEvent(st, m->up_ev[u], 0));
+            }
             CREST_TRY(compact_extract(m, proto, p->d, u0, u1, st));
             for (int64_t s0 = u0; s0 < u1; s0 += p->w.m_cap) {
                 const int64_t n = std::min(p->w.m_cap, u1 - s0);

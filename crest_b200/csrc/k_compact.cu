@@ -209,6 +209,7 @@ int launch_dup_compact(const int64_t *indptr, int64_t n_cells, const CompactHvg 
 // stored after a warp barrier -- the tile matches the CSR densify bit for
 // bit.  The colsum of S is privatised per block in shared memory.
 constexpr int kDensifyCWarps = 16;
+constexpr int kDensifyU = 8;  // entry loads in flight per lane
 
 template <int MODE> struct CElem;
 template <> struct CElem<0> { using T = double; };
@@ -267,9 +268,22 @@ __global__ void __launch_bounds__(kDensifyCWarps * 32) k_densify_compact(
         const double scale = in.scale[cell];
         const int64_t base = indptr[cell];
         E *row_lo = lo_plane + (size_t)i * d_pad;
-        for (int e = lane; e < n; e += 32) {
-            const int32_t sub = __ldcs(in.code + base + e);
-            const double s = scale_value(t, sub, transform_value(tc, scale, __ldcs(in.x + base + e)));
+        // the cell's entries in rounds of 32 x kDensifyU, every load of a
+        // round issued before the first is used
+        for (int e0 = 0; e0 < n; e0 += 32 * kDensifyU) {
+            int32_t subs[kDensifyU];
+            float xs[kDensifyU];
+#pragma unroll
+            for (int u = 0; u < kDensifyU; ++u) {
+                const int e = e0 + 32 * u + lane;
+                subs[u] = e < n ? __ldcs(in.code + base + e) : -1;
+                xs[u] = e < n ? __ldcs(in.x + base + e) : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < kDensifyU; ++u) {
+            const int32_t sub = subs[u];
+            if (sub < 0) continue;
+            const double s = scale_value(t, sub, transform_value(tc, scale, xs[u]));
             if (MODE == 0) {
                 row[sub] = s;
             } else {
@@ -287,6 +301,7 @@ __global__ void __launch_bounds__(kDensifyCWarps * 32) k_densify_compact(
                               (unsigned long long)__double2ll_rn(s * 4294967296.0));
                 else
                     atomicAdd(colsum + sub, s);
+            }
             }
         }
     }

@@ -39,7 +39,7 @@ namespace {
 
 constexpr int kJacobiMax = 160;
 constexpr int kJacobiSmemV = 112;  // V also kept in shared memory up to this size
-constexpr int kLanczos = 48;
+constexpr int kLanczos = 32;  // steps of the spectrum-bounds run
 
 // ------------------------------------------------------------ centring
 __global__ void k_centre(const double *__restrict__ G, const double *__restrict__ c, int64_t d, double n,
@@ -239,19 +239,27 @@ __global__ void k_gemm_reduce(Gemm g, int ksplit, const double *__restrict__ ws)
 // partials in slice order (distributed shared memory), so results do not
 // depend on scheduling.
 namespace dm {
-constexpr int kBM = 64, kBK = 16, kThreads = 256;
-constexpr int kAS = kBM + 4;  // A stage: [k][m], m stride 68
-constexpr int kBS = kBK + 4;  // B stage: [n][k], k stride 20
-constexpr int kAStage = kBM * kBS > kBK * kAS ? kBM * kBS : kBK * kAS;
+constexpr int kBK = 16;
+constexpr int kBS = kBK + 4;  // [n][k] (and A^T's [m][k]) staging: k stride 20
 constexpr int kMaxSplit = 16;
 
-template <int NF>
+// Tile shapes: WM x WN warps, each FM x FN fragments of 8 x 8; 4 x 2 warps of
+// 2 x NF fragments (tile 64 x 16 NF) with six, four and three stages for
+// NF = 1, 2, 4.  (Two by two warps of 4 x 4 fragments at 128 threads, three
+// CTAs per SM, measured 12 % slower on the 2000 x 2000 x 63 products.)
+template <int KIND>
 struct Cfg {
-    static constexpr int BN = 16 * NF;
-    static constexpr int ST = NF == 1 ? 6 : NF == 2 ? 4 : 3;
+    static constexpr int WM = 4, WN = 2;
+    static constexpr int FM = 2, FN = KIND == 0 ? 1 : KIND == 1 ? 2 : 4;
+    static constexpr int BM = WM * FM * 8, BN = WN * FN * 8;
+    static constexpr int THREADS = 32 * WM * WN;
+    static constexpr int ST = KIND == 0 ? 6 : KIND == 1 ? 4 : 3;
+    static constexpr int AS = BM + 4;  // A staging [k][m]: m stride, 4 mod 16
+    static constexpr int AStage = BM * kBS > kBK * AS ? BM * kBS : kBK * AS;
     static constexpr int BStage = BN * kBS;
-    static constexpr size_t smem = sizeof(double) * (size_t)ST * (kAStage + BStage);
-    static_assert((size_t)ST * (kAStage + BStage) >= (size_t)kBM * BN, "partial tile must fit the ring");
+    static constexpr size_t smem = sizeof(double) * (size_t)ST * (AStage + BStage);
+    static_assert((size_t)ST * (AStage + BStage) >= (size_t)BM * BN, "partial tile must fit the ring");
+    static_assert(AS % 16 == 4 && kBS % 16 == 4, "fragment loads must not conflict");
 };
 
 __device__ __forceinline__ void cp16(void *smem, const void *gmem, bool ok) {
@@ -279,29 +287,27 @@ __device__ __forceinline__ const double *cluster_ptr(const double *p, unsigned r
     return reinterpret_cast<const double *>(r);
 }
 
-template <int NF, bool TA>
-__global__ void __launch_bounds__(kThreads, 2) k_gemm_dmma(Gemm g, int kchunk) {
-    using C = Cfg<NF>;
-    constexpr int BN = C::BN, ST = C::ST;
+template <int KIND, bool TA>
+__global__ void __launch_bounds__(Cfg<KIND>::THREADS, 2) k_gemm_dmma(Gemm g, int kchunk) {
+    using C = Cfg<KIND>;
+    constexpr int BM = C::BM, BN = C::BN, ST = C::ST, FM = C::FM, FN = C::FN, T = C::THREADS;
     extern __shared__ __align__(16) double sm[];
-    double *As = sm, *Bs = sm + ST * kAStage;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp & 3, wn = warp >> 2;
-    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN;
+    double *As = sm, *Bs = sm + ST * C::AStage;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp % C::WM, wn = warp / C::WM;
+    const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
     const int kb = blockIdx.z * kchunk, ke = min(g.K, kb + kchunk);
     const int ntiles = ke > kb ? (ke - kb + kBK - 1) / kBK : 0;
 
     auto load = [&](int t, int stage) {
         const int k0 = kb + t * kBK;
-        double *as = As + stage * kAStage, *bs = Bs + stage * C::BStage;
-        // A: 16 k x 64 m = 512 chunks of two m ([k][m]), or of two k for A^T ([m][k])
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const int c = tid + r * kThreads;
+        double *as = As + stage * C::AStage, *bs = Bs + stage * C::BStage;
+        // A: 16 k x BM m in chunks of two m ([k][m]), or of two k for A^T ([m][k])
+        for (int c = tid; c < 8 * BM; c += T) {
             if (!TA) {
-                const int kk = c >> 5, mm = (c & 31) * 2;
+                const int kk = c / (BM / 2), mm = (c % (BM / 2)) * 2;
                 const int m = m0 + mm, k = k0 + kk;
                 const bool ok = m < g.M && k < ke;
-                cp16(as + kk * kAS + mm, ok ? g.A + m + (int64_t)k * g.lda : g.A, ok);
+                cp16(as + kk * C::AS + mm, ok ? g.A + m + (int64_t)k * g.lda : g.A, ok);
             } else {
                 const int mm = c >> 3, kk = (c & 7) * 2;
                 const int m = m0 + mm, k = k0 + kk;
@@ -309,8 +315,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_gemm_dmma(Gemm g, int kchunk) {
                 cp16(as + mm * kBS + kk, ok ? g.A + k + (int64_t)m * g.lda : g.A, ok);
             }
         }
-        // B: BN n x 16 k = 8 BN chunks of two k
-        for (int c = tid; c < 8 * BN; c += kThreads) {
+        // B: BN n x 16 k in chunks of two k
+        for (int c = tid; c < 8 * BN; c += T) {
             const int nn = c >> 3, kk = (c & 7) * 2;
             const int n = n0 + nn, k = k0 + kk;
             const bool ok = n < g.N && k < ke;
@@ -318,11 +324,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_gemm_dmma(Gemm g, int kchunk) {
         }
     };
 
-    double acc[2][NF][2];
+    double acc[FM][FN][2];
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < FM; ++i)
 #pragma unroll
-        for (int j = 0; j < NF; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int j = 0; j < FN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
 #pragma unroll
     for (int s = 0; s < ST - 1; ++s) {
@@ -336,19 +342,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_gemm_dmma(Gemm g, int kchunk) {
         if (t + ST - 1 < ntiles) load(t + ST - 1, (t + ST - 1) % ST);
         cp_commit();
         const double *as =
-            As + (t % ST) * kAStage + (TA ? (wm * 16 + ar) * kBS + ac : wm * 16 + ar + ac * kAS);
-        const double *bs = Bs + (t % ST) * C::BStage + (wn * 8 * NF + ar) * kBS + ac;
+            As + (t % ST) * C::AStage + (TA ? (wm * FM * 8 + ar) * kBS + ac : wm * FM * 8 + ar + ac * C::AS);
+        const double *bs = Bs + (t % ST) * C::BStage + (wn * FN * 8 + ar) * kBS + ac;
 #pragma unroll
         for (int k4 = 0; k4 < kBK; k4 += 4) {
-            double a[2], b[NF];
+            double a[FM], b[FN];
 #pragma unroll
-            for (int i = 0; i < 2; ++i) a[i] = TA ? as[i * 8 * kBS + k4] : as[k4 * kAS + i * 8];
+            for (int i = 0; i < FM; ++i) a[i] = TA ? as[i * 8 * kBS + k4] : as[k4 * C::AS + i * 8];
 #pragma unroll
-            for (int j = 0; j < NF; ++j) b[j] = bs[j * 8 * kBS + k4];
+            for (int j = 0; j < FN; ++j) b[j] = bs[j * 8 * kBS + k4];
 #pragma unroll
-            for (int i = 0; i < 2; ++i)
+            for (int i = 0; i < FM; ++i)
 #pragma unroll
-                for (int j = 0; j < NF; ++j) dmma(acc[i][j], a[i], b[j]);
+                for (int j = 0; j < FN; ++j) dmma(acc[i][j], a[i], b[j]);
         }
     }
     cp_wait<0>();
@@ -364,30 +370,31 @@ __global__ void __launch_bounds__(kThreads, 2) k_gemm_dmma(Gemm g, int kchunk) {
     const int ks = (int)gridDim.z;
     if (ks == 1) {
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < FM; ++i)
 #pragma unroll
-            for (int j = 0; j < NF; ++j)
+            for (int j = 0; j < FN; ++j)
 #pragma unroll
                 for (int h = 0; h < 2; ++h)
-                    out(m0 + wm * 16 + i * 8 + ar, n0 + wn * 8 * NF + j * 8 + ac * 2 + h, acc[i][j][h]);
+                    out(m0 + wm * FM * 8 + i * 8 + ar, n0 + wn * FN * 8 + j * 8 + ac * 2 + h, acc[i][j][h]);
         return;
     }
     // partial tile [m][n] in this CTA's ring, then the cluster-wide row split
     __syncthreads();
     double *part = sm;
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < FM; ++i)
 #pragma unroll
-        for (int j = 0; j < NF; ++j)
+        for (int j = 0; j < FN; ++j)
 #pragma unroll
             for (int h = 0; h < 2; ++h)
-                part[(wm * 16 + i * 8 + ar) * BN + wn * 8 * NF + j * 8 + ac * 2 + h] = acc[i][j][h];
+                part[(wm * FM * 8 + i * 8 + ar) * BN + wn * FN * 8 + j * 8 + ac * 2 + h] = acc[i][j][h];
     cluster_sync_all();
-    const int r = (int)blockIdx.z, rows = kBM / ks, e0 = r * rows * BN, e1 = e0 + rows * BN;
+    const int r = (int)blockIdx.z, rows = (BM + ks - 1) / ks;
+    const int e0 = min(BM, r * rows) * BN, e1 = min(BM, (r + 1) * rows) * BN;
     const double *src[kMaxSplit];
 #pragma unroll
     for (int z = 0; z < kMaxSplit; ++z) src[z] = z < ks ? cluster_ptr(part, (unsigned)z) : part;
-    for (int e = e0 + tid; e < e1; e += kThreads) {
+    for (int e = e0 + tid; e < e1; e += T) {
         double v = 0.0;
 #pragma unroll
         for (int z = 0; z < kMaxSplit; ++z)
@@ -416,22 +423,28 @@ static bool dmma_fits(const Gemm &g) {
            !(g.ldb & 1) && (g.tA || !(g.M & 1)) && al(g.A) && al(g.B);
 }
 
-template <int NF, bool TA>
-static int launch_dmma(const Gemm &g, int mt, int nt, int ks, int kchunk, cudaStream_t st) {
-    const void *fn = (const void *)dm::k_gemm_dmma<NF, TA>;
-    CREST_TRY(ensure_smem_attr(fn, dm::Cfg<NF>::smem));
+template <int KIND, bool TA>
+static int launch_dmma(const Gemm &g, cudaStream_t st) {
+    using C = dm::Cfg<KIND>;
+    const void *fn = (const void *)dm::k_gemm_dmma<KIND, TA>;
+    CREST_TRY(ensure_smem_attr(fn, C::smem));
     static bool nonportable = [fn] {
         const bool ok = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
         (void)cudaGetLastError();
         return ok;
     }();
-    if (!nonportable && ks > 8) ks = 8;
+    const int mt = (int)ceil_div(g.M, C::BM), nt = (int)ceil_div(g.N, C::BN);
+    // K split = the cluster's z extent: about two CTAs per SM, slices of at
+    // least 64, a power of two up to 16 (8 without non-portable clusters)
+    const int want = std::max(1, std::min((2 * device_sms()) / (mt * nt), g.K / (4 * dm::kBK)));
+    int ks = 1;
+    while (ks * 2 <= want && ks * 2 <= (nonportable ? dm::kMaxSplit : 8)) ks *= 2;
     auto launch = [&](int z) {
-        const int kc = z > 1 ? (int)round_up(ceil_div(g.K, z), dm::kBK) : kchunk;
+        const int kc = z > 1 ? (int)round_up(ceil_div(g.K, z), dm::kBK) : g.K;
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(mt, nt, z);
-        cfg.blockDim = dim3(dm::kThreads);
-        cfg.dynamicSmemBytes = dm::Cfg<NF>::smem;
+        cfg.blockDim = dim3(C::THREADS);
+        cfg.dynamicSmemBytes = C::smem;
         cfg.stream = st;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -440,29 +453,23 @@ static int launch_dmma(const Gemm &g, int mt, int nt, int ks, int kchunk, cudaSt
         attr[0].val.clusterDim.z = z;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, dm::k_gemm_dmma<NF, TA>, g, kc);
+        return cudaLaunchKernelEx(&cfg, dm::k_gemm_dmma<KIND, TA>, g, kc);
     };
     cudaError_t e = launch(ks);
-    if (e != cudaSuccess && ks > 8) {  // a 16-CTA cluster that cannot be placed: 8 slices
+    if (e != cudaSuccess && ks > 1) {  // a cluster shape that cannot be placed: a power of two up to 8
         (void)cudaGetLastError();
-        e = launch(8);
+        int z = 1;
+        while (z * 2 <= std::min(ks, 8)) z *= 2;
+        e = launch(z);
     }
     CREST_CUDA_TRY(e);
     return CREST_OK;
 }
 
-// K split: about two CTAs per SM, a power of two (the cluster extent) up to
-// 16, slices of at least 64.
 static int gemm_dmma(const Gemm &g, GemmWs &, cudaStream_t st) {
-    const int nf = g.N <= 16 ? 1 : g.N <= 32 ? 2 : 4;
-    const int mt = (int)ceil_div(g.M, dm::kBM), nt = (int)ceil_div(g.N, 16 * nf);
-    const int want = std::max(1, std::min((2 * device_sms()) / (mt * nt), g.K / (4 * dm::kBK)));
-    int ks = 1;
-    while (ks * 2 <= want && ks * 2 <= dm::kMaxSplit) ks *= 2;
-    const int kchunk = ks > 1 ? (int)round_up(ceil_div(g.K, ks), dm::kBK) : g.K;
-    if (nf == 1) return g.tA ? launch_dmma<1, true>(g, mt, nt, ks, kchunk, st) : launch_dmma<1, false>(g, mt, nt, ks, kchunk, st);
-    if (nf == 2) return g.tA ? launch_dmma<2, true>(g, mt, nt, ks, kchunk, st) : launch_dmma<2, false>(g, mt, nt, ks, kchunk, st);
-    return g.tA ? launch_dmma<4, true>(g, mt, nt, ks, kchunk, st) : launch_dmma<4, false>(g, mt, nt, ks, kchunk, st);
+    if (g.N <= 16) return g.tA ? launch_dmma<0, true>(g, st) : launch_dmma<0, false>(g, st);
+    if (g.N <= 32) return g.tA ? launch_dmma<1, true>(g, st) : launch_dmma<1, false>(g, st);
+    return g.tA ? launch_dmma<2, true>(g, st) : launch_dmma<2, false>(g, st);
 }
 
 int gemm(const Gemm &g, GemmWs &w, cudaStream_t st) {
@@ -1106,23 +1113,29 @@ __device__ __forceinline__ unsigned long long gtimer() {
     return t;
 }
 
-// Grid barrier on a counter that only grows (zeroed before the launch):
-// barrier number `phase` is passed once it reaches phase x nblk, so every CTA
-// arrives with one atomic and leaves as soon as it reads the total -- no
-// second round trip through a generation word.
-__device__ void grid_barrier(unsigned *count, unsigned &phase, unsigned nblk, int *err) {
+// Grid barrier on counters that only grow (zeroed before the launch).  CTAs
+// arrive on the counter of their group of 16 (one 128-byte line each, so
+// arrivals do not all queue on one address); the last arrival of a group
+// adds one to the top counter, and barrier number `phase` is passed once the
+// top counter reaches phase x groups.
+constexpr int kBarGroup = 16;
+
+__device__ void grid_barrier(unsigned *bar, unsigned &phase, unsigned nblk, int *err) {
     __syncthreads();
     ++phase;
     if (threadIdx.x == 0) {
         volatile int *e = err;
         if (!*e) {
-            const unsigned target = phase * nblk;
+            const unsigned n_groups = (nblk + kBarGroup - 1) / kBarGroup, g = blockIdx.x / kBarGroup;
+            const unsigned in_group = min((unsigned)kBarGroup, nblk - g * kBarGroup);
+            unsigned *top = bar, *mine = bar + 32 * (1 + g);
             __threadfence();
-            atomicAdd(count, 1u);
+            if (atomicAdd(mine, 1u) == phase * in_group - 1) atomicAdd(top, 1u);
+            const unsigned target = phase * n_groups;
             const unsigned long long t0 = gtimer();
             for (;;) {
                 unsigned v;
-                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+                asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(top) : "memory");
                 if (v >= target) break;
                 if (*e || gtimer() - t0 > 1000000000ull) {
                     atomicExch(err, 1);
@@ -1305,8 +1318,10 @@ int lanczos_coop(EigWork &w, const double *C, int64_t d, int L, cudaStream_t st)
     }
     CREST_TRY(w.lw2.ensure(sizeof(double) * (size_t)d));
     CREST_TRY(w.lpart.ensure(sizeof(double) * (size_t)nb * 3 * (kLanczos + 1)));
-    CREST_TRY(w.lbar.ensure(sizeof(unsigned) * 2));
-    CREST_CUDA_TRY(cudaMemsetAsync(w.lbar.ptr, 0, sizeof(unsigned) * 2, st));
+    // the top counter, then one 128-byte line per group of CTAs
+    const size_t bar_bytes = sizeof(unsigned) * 32 * (1 + (size_t)ceil_div(nb, kBarGroup));
+    CREST_TRY(w.lbar.ensure(bar_bytes));
+    CREST_CUDA_TRY(cudaMemsetAsync(w.lbar.ptr, 0, bar_bytes, st));
     CREST_CUDA_TRY(cudaMemsetAsync(w.fail.as<int>() + 3, 0, sizeof(int), st));
     LanczosArgs a{C, d, L, rows, w.lz.as<double>(), w.lw2.as<double>(), w.lpart.as<double>(),
                   w.lab.as<double>(), w.lbar.as<unsigned>(), w.fail.as<int>() + 3};

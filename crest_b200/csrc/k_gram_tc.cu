@@ -669,7 +669,9 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_pair(const __grid_constant
             double *G = half == 0 ? a.G : a.G_aux;
             const double nk = (double)*a.n_kept;
             // two rows per pass, every load of a pass issued before the
-            // first add: 16 independent G reads in flight per lane
+            // first add: 16 independent G reads in flight per lane; G goes
+            // through L2 as evict-first so that it does not push the next
+            // tile's operands out
             for (int r0 = e; r0 < kHalfRows; r0 += 2 * kEpiWarps) {
                 double gv[2][8];
 #pragma unroll
@@ -678,7 +680,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_pair(const __grid_constant
 #pragma unroll
                     for (int c = 0; c < 8; ++c) {
                         const int64_t gb = (int64_t)bj * kN + lane + 32 * c;
-                        gv[u][c] = (ga < a.d && gb < a.d && gb >= ga) ? G[ga * a.d + gb] : 0.0;
+                        gv[u][c] = (ga < a.d && gb < a.d && gb >= ga) ? __ldcs(G + ga * a.d + gb) : 0.0;
                     }
                 }
 #pragma unroll
@@ -694,7 +696,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_pair(const __grid_constant
                         if (gb >= a.d || gb < ga) continue;
                         double v = (double)stage[r * kPitch + cc];
                         if (corr) v = v - ba * a.colsum[gb] - ca * a.bias[gb] - nk * ba * a.bias[gb];
-                        G[ga * a.d + gb] = gv[u][c] + v;
+                        __stcs(G + ga * a.d + gb, gv[u][c] + v);
                     }
                 }
             }

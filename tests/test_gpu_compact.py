@@ -64,22 +64,23 @@ def test_plan_fp64_gram_bit_exact(small_counts, residency):
     dm.close()
 
 
-def test_compact_projection_equals_csr_projection(small_counts):
+@pytest.mark.parametrize("k", [20, 50])
+def test_compact_projection_equals_csr_projection(small_counts, k):
     """The same plan (same loadings) projects a device-resident matrix from the
     compact form and a streamed one from the CSR: identical scores."""
     s = setup(small_counts, 4)
     p, dm, scale = plan_gram(s, "device")
-    p.solve(s["nr"], 20)
+    p.solve(s["nr"], k)
     Xa = p.project(dm, s["cm"], s["gm"], 1e4, True, s["sub"], s["nv"], scale, s["nr"])
     dh = DeviceMatrix(s["indptr"], s["indices"], s["data"], s["n_genes"], "host", chunk_cells=300)
     Xb = p.project(dh, s["cm"], s["gm"], 1e4, True, s["sub"], s["nv"], scale, s["nr"])
     assert np.array_equal(Xa, Xb)
     # and the oracle's projection with the plan's loadings adds the same per-cell sums
     L = p.results()[1]
-    Xo = np.zeros((s["nr"], 20), np.float32)
+    Xo = np.zeros((s["nr"], k), np.float32)
     oracle.project(s["indices"], s["data"], s["cm"], s["gm"], 1e4, True, None, s["indptr"], 0, s["sub"], L, Xo,
                    True, s["mean"], s["std"], 10.0)
-    Xz = np.zeros((s["nr"], 20), np.float32)
+    Xz = np.zeros((s["nr"], k), np.float32)
     _native.project(s["indices"], s["data"], s["cm"], s["gm"], 1e4, True, None, s["indptr"], 0, s["sub"], L, Xz,
                     True, s["mean"], s["std"], 10.0)
     assert np.array_equal(Xz, Xo)
