@@ -57,6 +57,7 @@ class Synth(C.Structure):
 _SIGS = {
     "crest_version": [],
     "crest_device_count": [],
+    "crest_memory_stats": [C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.c_int32],
     "crest_set_device": [C.c_int],
     "crest_qc": [P, P, I64, P, P, P, I64, P, P],
     "crest_qc_static": [P, P, I64, P, P, P, I64, P, P],
@@ -175,3 +176,10 @@ def carray(a, dtype, name):
     if not a.flags.c_contiguous:
         raise ValueError(f"{name} must be C-contiguous")
     return a
+
+
+def memory_stats(reset_high: bool = False):
+    """(bytes in use, high-water mark) of the library's device allocations."""
+    u, h = C.c_int64(), C.c_int64()
+    call("crest_memory_stats", C.byref(u), C.byref(h), int(bool(reset_high)))
+    return u.value, h.value

@@ -43,7 +43,7 @@ static bool injected_alloc_failure() {
 }
 
 // The library's memory pool of the current device (nullptr: none).
-static cudaMemPool_t device_pool() {
+cudaMemPool_t device_pool() {
     static std::mutex mu;
     static cudaMemPool_t pools[64];
     static bool tried[64];
@@ -359,6 +359,23 @@ extern "C" {
 
 const char *crest_last_error(void) { return last_error(); }
 int crest_version(void) { return 1; }
+
+int crest_memory_stats(int64_t *used, int64_t *used_high, int32_t reset_high) {
+    CREST_TRY(crest::require_device());
+    cudaMemPool_t pool = crest::device_pool();
+    uint64_t u = 0, h = 0;
+    if (pool) {
+        CREST_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &u));
+        CREST_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &h));
+        if (reset_high) {
+            uint64_t zero = 0;
+            CREST_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &zero));
+        }
+    }
+    if (used) *used = (int64_t)u;
+    if (used_high) *used_high = (int64_t)h;
+    return CREST_OK;
+}
 
 int crest_device_count(void) {
     int n = 0;

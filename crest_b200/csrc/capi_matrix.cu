@@ -56,6 +56,11 @@ struct crest_matrix {
     // buffers could not be allocated (the passes then read the CSR)
     crest::DevBuf cmp_code, cmp_x, cmp_n, cmp_scale, cmp_status, cls;
     bool compact_off = false, cmp_valid = false;
+    // streamed matrices: the compact form packed at running offsets (cmp_off)
+    // through a chunk-sized scratch; cmp_packed marks that layout
+    crest::DevBuf cmp_off, cmp_sc, cmp_sx, cmp_total;
+    bool cmp_packed = false;
+    int64_t cmp_cap = 0;
     std::vector<int64_t> cmp_cell_map;
     std::vector<int32_t> cmp_gene_map, cmp_sub_map;
     double cmp_target = 0.0;
@@ -305,8 +310,52 @@ CompactHvg compact_view(crest_matrix *m) {
 }
 
 void compact_release(crest_matrix *m) {
-    for (auto *b : {&m->cmp_code, &m->cmp_x, &m->cmp_n, &m->cmp_scale, &m->cmp_status, &m->cls}) b->release();
+    for (auto *b : {&m->cmp_code, &m->cmp_x, &m->cmp_n, &m->cmp_scale, &m->cmp_status, &m->cls, &m->cmp_off,
+                    &m->cmp_sc, &m->cmp_sx, &m->cmp_total})
+        b->release();
     m->cmp_valid = false;
+}
+
+// Buffers of the packed compact form of a streamed matrix: room for a
+// quarter of the stored entries (HVG entries are about one in eight for
+// 2,000 of 30,000+ genes); compact_off when they do not fit.
+int streamed_compact_prepare(crest_matrix *m, int64_t d, bool &ok, cudaStream_t st) {
+    ok = false;
+    m->cmp_valid = false;
+    if (m->residency != CREST_MEM_HOST || m->compact_off || m->n_cells == 0) return CREST_OK;
+    if (4 * gene_class_words(std::max<int64_t>(m->n_genes, 1)) > (size_t)kMaxSmem) return CREST_OK;
+    const char *e = getenv("CREST_STREAM_COMPACT");  // 0: the projection streams the CSR again
+    if (e && e[0] == '0') return CREST_OK;
+    int64_t piece_max = 1;
+    for (int64_t s0 = 0; s0 < m->n_cells; s0 += m->chunk_cells) {
+        const int64_t s1 = std::min(m->n_cells, s0 + m->chunk_cells);
+        piece_max = std::max(piece_max, m->h_indptr[s1] - m->h_indptr[s0]);
+    }
+    m->cmp_cap = m->nnz / 4 + 1024;
+    const size_t n = (size_t)m->n_cells;
+    if (m->cmp_code.ensure(4 * (size_t)m->cmp_cap) || m->cmp_x.ensure(4 * (size_t)m->cmp_cap) ||
+        m->cmp_n.ensure(4 * n) || m->cmp_scale.ensure(8 * n) || m->cmp_off.ensure(8 * n) ||
+        m->cmp_status.ensure(sizeof(int)) || m->cmp_total.ensure(8) || m->cmp_sc.ensure(4 * (size_t)piece_max) ||
+        m->cmp_sx.ensure(4 * (size_t)piece_max) || m->cls.ensure(4 * gene_class_words(std::max<int64_t>(m->n_genes, 1)))) {
+        compact_release(m);
+        cudaGetLastError();
+        m->compact_off = true;
+        return CREST_OK;
+    }
+    CREST_TRY(launch_gene_class(m->code.as<int32_t>(), m->n_genes, d, m->cls.as<uint32_t>(), st));
+    CREST_CUDA_TRY(cudaMemsetAsync(m->cmp_status.ptr, 0, sizeof(int), st));
+    CREST_CUDA_TRY(cudaMemsetAsync(m->cmp_total.ptr, 0, 8, st));
+    ok = true;
+    return CREST_OK;
+}
+
+// One streamed chunk: its compact form into the scratch, then packed.
+int streamed_compact_chunk(crest_matrix *m, const DevChunk &c, int64_t d, cudaStream_t st) {
+    const CompactHvg scratch{m->cmp_sc.as<int32_t>(), m->cmp_sx.as<float>(), m->cmp_n.as<int32_t>(),
+                             m->cmp_scale.as<double>(), m->cmp_status.as<int>()};
+    CREST_TRY(launch_extract(c, m->cls.as<uint32_t>(), m->code.as<int32_t>(), d, scratch, st));
+    return launch_compact_pack(c, scratch, compact_view(m), m->cmp_off.as<int64_t>(),
+                               m->cmp_total.as<unsigned long long>(), m->cmp_cap, st);
 }
 
 // One read of the device-resident CSR into the compact HVG form (k_extract);
@@ -720,6 +769,7 @@ int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
     CREST_TRY(gram_status_reset(p->w, st));
     bool compact = false;
     CREST_TRY(compact_pass(m, proto, p->d, compact, st));
+    if (compact) m->cmp_packed = false;
     if (compact) {  // per upload chunk: its compact HVG form, then its Gram tiles
         const CompactHvg ch = compact_view(m);
         int64_t u0 = 0;
@@ -741,15 +791,25 @@ int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
         m->up_waited = true;
     } else {
         CREST_TRY(wait_upload(m));
+        bool packed = false;  // streamed: also keep the packed compact form for the projection
+        CREST_TRY(streamed_compact_prepare(m, p->d, packed, st));
         CREST_TRY(for_each_piece(m, proto, p->w.m_cap, [&](const DevChunk &c) {
-            return gram_over_chunk(c, m->code.as<int32_t>(), ds, p->w, p->gram.as<double>(), p->colsum.as<double>(),
-                                   st);
+            CREST_TRY(gram_over_chunk(c, m->code.as<int32_t>(), ds, p->w, p->gram.as<double>(),
+                                      p->colsum.as<double>(), st));
+            return packed ? streamed_compact_chunk(m, c, p->d, st) : CREST_OK;
         }));
+        if (packed) {
+            int h = 0;
+            CREST_CUDA_TRY(cudaMemcpyAsync(&h, m->cmp_status.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+            CREST_CUDA_TRY(cudaStreamSynchronize(st));
+            compact = !(h & 8);  // every cell's entries fitted: the projection reads the packed form
+            m->cmp_packed = compact;
+        }
     }
     CREST_TRY(gram_aux_fold(p->w, p->gram.as<double>(), st));
     p->stats.gram_ms = t.stop();
     CREST_CUDA_TRY(cudaGetLastError());
-    if (compact) CREST_TRY(compact_dup_check(m, p->d, st));
+    if (compact && !m->cmp_packed) CREST_TRY(compact_dup_check(m, p->d, st));
     CREST_TRY(gram_status_check(p->w, st));
     if (p->precision == CREST_GRAM_BF16X3) CREST_TRY(tc_check_error());
     if (compact) {  // the projection of the same maps reads this form
@@ -855,9 +915,9 @@ int crest_pca_project(crest_pca *p, crest_matrix *m, const int64_t *cell_map, co
     CREST_CUDA_TRY(cudaGetLastError());
     const DevChunk proto = base_chunk(m, target_sum, log1p);
     if (compact_matches(m, cell_map, gene_map, sub_map, n_vars, target_sum, p->d)) {
-        CREST_TRY(launch_project_compact(m->d_indptr.as<int64_t>(), m->n_cells, m->cell_map.as<int64_t>(),
-                                         compact_view(m), target_sum, log1p, ds, p->vecs.as<double>(), (int)p->k, X,
-                                         st));
+        const int64_t *start = m->cmp_packed ? m->cmp_off.as<int64_t>() : m->d_indptr.as<int64_t>();
+        CREST_TRY(launch_project_compact(start, m->n_cells, m->cell_map.as<int64_t>(), compact_view(m), target_sum,
+                                         log1p, ds, p->vecs.as<double>(), (int)p->k, p->d, X, st));
     } else {
         CREST_TRY(stage_hvg_code(proto, m->sub_map.as<int32_t>(), n_vars, p->d, m->code, st));
         CREST_TRY(m->counter.ensure(sizeof(unsigned int)));

@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(kExtractWarps * 32, 4) k_extract(DevChunk c, c
 int launch_extract(const DevChunk &c, const uint32_t *cls, const int32_t *code, int64_t d, const CompactHvg &out,
                    cudaStream_t st) {
     if (c.n_spans == 0) return CREST_OK;
-    CREST_REQUIRE(c.base == 0 && !c.span_cell, CREST_EINVAL, "extract needs a whole CSR matrix");
+    CREST_REQUIRE(!c.span_cell, CREST_EINVAL, "extract needs CSR chunks");
     const size_t smem = 4 * gene_class_words(c.n_gene_map);
     CREST_REQUIRE(smem <= (size_t)kMaxSmem, CREST_EINVAL, "too many genes for the class table");
     CREST_TRY(ensure_smem_attr((const void *)k_extract<1>, smem));
@@ -373,11 +373,16 @@ int launch_densify_compact(const int64_t *indptr, int64_t cell0, int64_t n, cons
 
 // ------------------------------------------------------------ project
 // Warp per cell: the cell's compact entries are transformed in rounds of
-// kPCStage (lanes in parallel, staged in shared memory), then added in entry
+// STAGE (lanes in parallel, staged in shared memory), then added in entry
 // order into KPL f64 accumulators per lane (component lane + 32 q), the V
 // rows of U entries loaded before their ordered additions -- the same f64
 // operations in the same order as src/kernels.rs:360-369, so the scores are
 // bit-identical to the CSR projection.
+//
+// (Keeping the loadings rows of the most frequent columns in shared memory --
+// one 1,024-thread CTA per SM instead of four 512-thread ones -- measured
+// 7.5 ms against 5.1 ms at 1M cells: the pass is bound by each warp's
+// dependent chains, not by the L2 reads of V.)
 constexpr int kPCWarps = 16;
 constexpr int kPCStage = 256;
 
@@ -387,14 +392,15 @@ __global__ void __launch_bounds__(kPCWarps * 32) k_project_compact(const int64_t
                                                                    CompactHvg in, double target_sum, int log1p,
                                                                    DevScale t, const double *__restrict__ V, int k,
                                                                    float *__restrict__ out) {
-    constexpr int U = KPL >= 2 ? 4 : 8;
-    __shared__ double s_val[kPCWarps][kPCStage];
-    __shared__ int32_t s_code[kPCWarps][kPCStage];
+    constexpr int U = KPL >= 2 ? 4 : 8, WARPS = kPCWarps, STAGE = kPCStage;
+    __shared__ double s_val[WARPS][STAGE];
+    __shared__ int32_t s_code[WARPS][STAGE];
+    auto vrow = [&](int32_t c) -> const double * { return V + (size_t)c * k; };
     const int lane = lane_id(), wid = threadIdx.x >> 5;
     double *q_val = s_val[wid];
     int32_t *q_code = s_code[wid];
-    const int64_t warp = (int64_t)blockIdx.x * kPCWarps + wid;
-    const int64_t n_warps = (int64_t)gridDim.x * kPCWarps;
+    const int64_t warp = (int64_t)blockIdx.x * WARPS + wid;
+    const int64_t n_warps = (int64_t)gridDim.x * WARPS;
     DevChunk tc;
     tc.target_sum = target_sum;
     tc.log1p = log1p;
@@ -407,8 +413,8 @@ __global__ void __launch_bounds__(kPCWarps * 32) k_project_compact(const int64_t
         double acc[KPL];
 #pragma unroll
         for (int q = 0; q < KPL; ++q) acc[q] = 0.0;
-        for (int r0 = 0; r0 < n; r0 += kPCStage) {
-            const int m = n - r0 < kPCStage ? n - r0 : kPCStage;
+        for (int r0 = 0; r0 < n; r0 += STAGE) {
+            const int m = n - r0 < STAGE ? n - r0 : STAGE;
             __syncwarp();
             for (int e = lane; e < m; e += 32) {
                 const int32_t sub = __ldcs(in.code + base + r0 + e);
@@ -421,11 +427,11 @@ __global__ void __launch_bounds__(kPCWarps * 32) k_project_compact(const int64_t
                 double vv[U][KPL];
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
-                    const double *vr = V + (size_t)q_code[e + u] * k;
+                    const double *vr = vrow(q_code[e + u]);
 #pragma unroll
                     for (int q = 0; q < KPL; ++q) {
                         const int j = lane + 32 * q;
-                        vv[u][q] = j < k ? __ldg(vr + j) : 0.0;
+                        vv[u][q] = j < k ? vr[j] : 0.0;
                     }
                 }
 #pragma unroll
@@ -436,12 +442,12 @@ __global__ void __launch_bounds__(kPCWarps * 32) k_project_compact(const int64_t
                 }
             }
             for (; e < m; ++e) {
-                const double *vr = V + (size_t)q_code[e] * k;
+                const double *vr = vrow(q_code[e]);
                 const double sv = q_val[e];
 #pragma unroll
                 for (int q = 0; q < KPL; ++q) {
                     const int j = lane + 32 * q;
-                    if (j < k) acc[q] = __dadd_rn(acc[q], __dmul_rn(sv, __ldg(vr + j)));
+                    if (j < k) acc[q] = __dadd_rn(acc[q], __dmul_rn(sv, vr[j]));
                 }
             }
         }
@@ -468,14 +474,103 @@ static int project_compact_k(const int64_t *indptr, int64_t n_cells, const int64
 }
 
 int launch_project_compact(const int64_t *indptr, int64_t n_cells, const int64_t *cell_map, const CompactHvg &in,
-                           double target_sum, int log1p, const DevScale &t, const double *V, int k, float *out,
-                           cudaStream_t st) {
+                           double target_sum, int log1p, const DevScale &t, const double *V, int k, int64_t d,
+                           float *out, cudaStream_t st) {
     if (n_cells == 0 || k == 0) return CREST_OK;
     CREST_REQUIRE(k <= 128, CREST_EINVAL, "project supports k <= 128 (got %d)", k);
+    (void)d;
     prof::Scope ps("project_compact", st);
     if (k <= 32) return project_compact_k<1>(indptr, n_cells, cell_map, in, target_sum, log1p, t, V, k, out, st);
     if (k <= 64) return project_compact_k<2>(indptr, n_cells, cell_map, in, target_sum, log1p, t, V, k, out, st);
     return project_compact_k<4>(indptr, n_cells, cell_map, in, target_sum, log1p, t, V, k, out, st);
+}
+
+}  // namespace crest
+
+namespace crest {
+
+// ------------------------------------- compact form of a streamed matrix
+// A streamed (host-resident) matrix has no CSR on the device to hold the
+// compact form in place, so each chunk is extracted into a chunk-sized
+// scratch (cell slots as in its chunk buffer) and the cells' HVG entries are
+// then packed into one device array at running offsets: off[cell] = the
+// entries of all earlier cells.  *total carries the offset from chunk to
+// chunk; a cell whose entries would pass `cap` sets bit 3 of *status and is
+// left out (the caller then projects from the CSR instead).
+
+// Exclusive scan of the chunk's entry counts (one CTA, cells [c0, c0 + n)).
+__global__ void __launch_bounds__(1024) k_compact_offsets(const int32_t *__restrict__ cnt, int64_t c0, int64_t n,
+                                                          int64_t *__restrict__ off,
+                                                          unsigned long long *__restrict__ total, int64_t cap,
+                                                          int *__restrict__ status) {
+    __shared__ long long warp_sums[32];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int64_t per = (n + blockDim.x - 1) / blockDim.x, i0 = min(n, (int64_t)tid * per), i1 = min(n, i0 + per);
+    long long mine = 0;
+    for (int64_t i = i0; i < i1; ++i) mine += max(cnt[c0 + i], 0);
+    long long incl = mine;  // inclusive scan over the block
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long v = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_sums[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        long long w = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long v = __shfl_up_sync(kFull, w, o);
+            if (lane >= o) w += v;
+        }
+        warp_sums[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    const long long base = (long long)*total;
+    long long run = base + (wid ? warp_sums[wid - 1] : 0) + incl - mine;
+    for (int64_t i = i0; i < i1; ++i) {
+        off[c0 + i] = run;
+        run += max(cnt[c0 + i], 0);
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const long long end = base + warp_sums[((blockDim.x >> 5)) - 1];
+        if (end > cap) atomicOr(status, 8);
+        *total = (unsigned long long)end;
+    }
+}
+
+// Warp per cell: its n entries from the chunk scratch (slot at
+// span_ptr[i] - base) to the packed array at off[cell].
+__global__ void __launch_bounds__(256) k_compact_move(const int64_t *__restrict__ span_ptr, int64_t base, int64_t c0,
+                                                      int64_t n, const int32_t *__restrict__ cnt,
+                                                      const int64_t *__restrict__ off, const int32_t *__restrict__ sc,
+                                                      const float *__restrict__ sx, int32_t *__restrict__ dc,
+                                                      float *__restrict__ dx, int64_t cap) {
+    const int lane = lane_id();
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        const int m = cnt[c0 + i];
+        if (m <= 0) continue;
+        const int64_t o = off[c0 + i], s = span_ptr[i] - base;
+        if (o + m > cap) continue;
+        for (int e = lane; e < m; e += 32) {
+            dc[o + e] = sc[s + e];
+            dx[o + e] = sx[s + e];
+        }
+    }
+}
+
+int launch_compact_pack(const DevChunk &c, const CompactHvg &scratch, const CompactHvg &packed, int64_t *off,
+                        unsigned long long *total, int64_t cap, cudaStream_t st) {
+    if (c.n_spans == 0) return CREST_OK;
+    k_compact_offsets<<<1, 1024, 0, st>>>(packed.n, c.first_cell, c.n_spans, off, total, cap, packed.status);
+    CREST_CUDA_TRY(cudaGetLastError());
+    const int64_t blocks = std::min<int64_t>(ceil_div(c.n_spans, 8), (int64_t)device_sms() * 8);
+    k_compact_move<<<(unsigned)blocks, 256, 0, st>>>(c.span_ptr, c.base, c.first_cell, c.n_spans, packed.n, off,
+                                                     scratch.code, scratch.x, packed.code, packed.x, cap);
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
 }
 
 }  // namespace crest

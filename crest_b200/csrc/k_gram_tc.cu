@@ -668,14 +668,15 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_pair(const __grid_constant
             const bool corr = half == 0 && a.bias;
             double *G = half == 0 ? a.G : a.G_aux;
             const double nk = (double)*a.n_kept;
-            // two rows per pass, every load of a pass issued before the
-            // first add: 16 independent G reads in flight per lane; G goes
-            // through L2 as evict-first so that it does not push the next
-            // tile's operands out
-            for (int r0 = e; r0 < kHalfRows; r0 += 2 * kEpiWarps) {
-                double gv[2][8];
+            // kRmwRows rows per pass, every load of a pass issued before the
+            // first add: 8 kRmwRows independent G reads in flight per lane;
+            // G goes through L2 as evict-first so that it does not push the
+            // next tile's operands out
+            constexpr int kRmwRows = 4;
+            for (int r0 = e; r0 < kHalfRows; r0 += kRmwRows * kEpiWarps) {
+                double gv[kRmwRows][8];
 #pragma unroll
-                for (int u = 0; u < 2; ++u) {
+                for (int u = 0; u < kRmwRows; ++u) {
                     const int64_t ga = (int64_t)bi * kN + (int64_t)rank * kHalfRows + r0 + u * kEpiWarps;
 #pragma unroll
                     for (int c = 0; c < 8; ++c) {
@@ -684,7 +685,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_syrk_pair(const __grid_constant
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < 2; ++u) {
+                for (int u = 0; u < kRmwRows; ++u) {
                     const int r = r0 + u * kEpiWarps;
                     const int64_t ga = (int64_t)bi * kN + (int64_t)rank * kHalfRows + r;
                     if (ga >= a.d) continue;

@@ -165,10 +165,17 @@ int launch_dup_compact(const int64_t *indptr, int64_t n_cells, const CompactHvg 
 // Densify cells [cell0, cell0 + n) of the compact form into the Gram tile.
 int launch_densify_compact(const int64_t *indptr, int64_t cell0, int64_t n, const CompactHvg &in, double target_sum,
                            int log1p, const DevScale &t, const GramWork &w, cudaStream_t st);
-// out[cell_map[i]] += scores of cell i (bit-identical to launch_project).
+// Streamed matrices: the HVG entries of chunk c (extracted into `scratch`,
+// slots as in the chunk buffer) packed into `packed` at running offsets
+// off[cell]; *total is the running entry count (bit 3 of *packed.status when
+// it would pass cap).
+int launch_compact_pack(const DevChunk &c, const CompactHvg &scratch, const CompactHvg &packed, int64_t *off,
+                        unsigned long long *total, int64_t cap, cudaStream_t st);
+// out[cell_map[i]] += scores of cell i (bit-identical to launch_project);
+// cell i's entries start at start[i] (indptr, or the packed offsets).
 int launch_project_compact(const int64_t *indptr, int64_t n_cells, const int64_t *cell_map, const CompactHvg &in,
-                           double target_sum, int log1p, const DevScale &t, const double *V, int k, float *out,
-                           cudaStream_t st);
+                           double target_sum, int log1p, const DevScale &t, const double *V, int k, int64_t d,
+                           float *out, cudaStream_t st);
 
 // ------------------------------------------------------------ eigensolver
 struct EigStats {

@@ -98,6 +98,12 @@ typedef struct crest_pca_stats {
 
 const char *crest_last_error(void);
 int crest_version(void);
+/* Device memory held by the library's allocations on the current device:
+ * bytes in use now and the high-water mark since the last reset (reset_high
+ * != 0 resets it after reading).  Buffers come from a stream-ordered pool
+ * that keeps freed memory for reuse, so the driver's free-memory figure
+ * does not show a call's working set. */
+int crest_memory_stats(int64_t *used, int64_t *used_high, int32_t reset_high);
 /* Number of CUDA devices (0 without a driver); never fails. */
 int crest_device_count(void);
 /* Select the device used by this thread's subsequent calls. */

@@ -73,8 +73,16 @@ def test_compact_projection_equals_csr_projection(small_counts, k):
     p.solve(s["nr"], k)
     Xa = p.project(dm, s["cm"], s["gm"], 1e4, True, s["sub"], s["nv"], scale, s["nr"])
     dh = DeviceMatrix(s["indptr"], s["indices"], s["data"], s["n_genes"], "host", chunk_cells=300)
-    Xb = p.project(dh, s["cm"], s["gm"], 1e4, True, s["sub"], s["nv"], scale, s["nr"])
+    Xb = p.project(dh, s["cm"], s["gm"], 1e4, True, s["sub"], s["nv"], scale, s["nr"])  # CSR streamed again
     assert np.array_equal(Xa, Xb)
+    # a streamed matrix whose Gram pass packed its compact form projects from it: the same scores
+    p2, dh2, _ = plan_gram(s, "host")
+    p2.solve(s["nr"], k)
+    assert np.array_equal(p2.results()[1], p.results()[1])
+    Xc = p2.project(dh2, s["cm"], s["gm"], 1e4, True, s["sub"], s["nv"], scale, s["nr"])
+    assert np.array_equal(Xa, Xc)
+    p2.close()
+    dh2.close()
     # and the oracle's projection with the plan's loadings adds the same per-cell sums
     L = p.results()[1]
     Xo = np.zeros((s["nr"], k), np.float32)
