@@ -41,8 +41,10 @@ struct crest_matrix {
     crest::DevBuf cell_map, gene_map, flag, sub_map, code, counter, mean, std_, bias;
     crest::DevBuf out[5];
     // gene-range index of a device-resident matrix (built on first use):
-    // range_state 0 = not built, 1 = rows sorted (index valid), -1 = unsorted
+    // range_state 0 = not built, 1 = rows sorted (index valid), -1 = unsorted;
+    // rows_strict: sorted with no gene id stored twice in a row
     int range_state = 0;
+    bool rows_strict = false;
     int range_log2_s = 12, n_ranges = 0;
     crest::DevBuf range_off, status;
     int qc_integral = 1;  // cleared once the QC sweep meets a non-integral value
@@ -246,8 +248,9 @@ int range_index(crest_matrix *m, RangeIndex &ix, bool &ok) {
         CREST_CUDA_TRY(cudaMemcpyAsync(&unsorted, m->status.ptr, sizeof(int), cudaMemcpyDeviceToHost, m->compute));
         CREST_CUDA_TRY(cudaStreamSynchronize(m->compute));
         m->n_ranges = R;
-        m->range_state = unsorted ? -1 : 1;
-        if (unsorted) m->range_off.release();
+        m->range_state = (unsorted & 1) ? -1 : 1;
+        m->rows_strict = unsorted == 0;
+        if (unsorted & 1) m->range_off.release();
     }
     if (m->range_state != 1) return CREST_OK;
     ix.log2_s = m->range_log2_s;
@@ -353,7 +356,7 @@ int streamed_compact_prepare(crest_matrix *m, int64_t d, bool &ok, cudaStream_t 
 int streamed_compact_chunk(crest_matrix *m, const DevChunk &c, int64_t d, cudaStream_t st) {
     const CompactHvg scratch{m->cmp_sc.as<int32_t>(), m->cmp_sx.as<float>(), m->cmp_n.as<int32_t>(),
                              m->cmp_scale.as<double>(), m->cmp_status.as<int>()};
-    CREST_TRY(launch_extract(c, m->cls.as<uint32_t>(), m->code.as<int32_t>(), d, scratch, st));
+    CREST_TRY(launch_extract(c, m->cls.as<uint32_t>(), m->code.as<int32_t>(), d, scratch, true, st));
     return launch_compact_pack(c, scratch, compact_view(m), m->cmp_off.as<int64_t>(),
                                m->cmp_total.as<unsigned long long>(), m->cmp_cap, st);
 }
@@ -385,7 +388,8 @@ int compact_pass(crest_matrix *m, const DevChunk &proto, int64_t d, bool &done, 
 
 // Compact form of cells [c0, c1) (after compact_pass), once the upload
 // chunk(s) holding them are on the device.
-int compact_extract(crest_matrix *m, const DevChunk &proto, int64_t d, int64_t c0, int64_t c1, cudaStream_t st) {
+int compact_extract(crest_matrix *m, const DevChunk &proto, int64_t d, int64_t c0, int64_t c1, bool check_order,
+                    cudaStream_t st) {
     DevChunk c = proto;
     c.genes = m->d_indices.as<uint32_t>();
     c.values = m->d_data.as<float>();
@@ -393,7 +397,20 @@ int compact_extract(crest_matrix *m, const DevChunk &proto, int64_t d, int64_t c
     c.first_cell = (uint32_t)c0;
     c.base = 0;
     c.n_spans = c1 - c0;
-    return launch_extract(c, m->cls.as<uint32_t>(), m->code.as<int32_t>(), d, compact_view(m), st);
+    return launch_extract(c, m->cls.as<uint32_t>(), m->code.as<int32_t>(), d, compact_view(m), check_order, st);
+}
+
+// True when the HVG column of a store gene (sub_map[gene_map[g]], as
+// launch_hvg_code forms it) strictly increases with g over the HVG genes.
+bool columns_monotone(const int32_t *gene_map, int64_t n_genes, const int32_t *sub_map, int64_t n_vars) {
+    int32_t last = -1;
+    for (int64_t g = 0; g < n_genes; ++g) {
+        const int32_t k = gene_map[g];
+        if (k < 0 || k >= n_vars || sub_map[k] < 0) continue;
+        if (sub_map[k] <= last) return false;
+        last = sub_map[k];
+    }
+    return true;
 }
 
 // Duplicate-column check of the compact form: only cells whose columns were
@@ -772,6 +789,13 @@ int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
     if (compact) m->cmp_packed = false;
     if (compact) {  // per upload chunk: its compact HVG form, then its Gram tiles
         const CompactHvg ch = compact_view(m);
+        // the zero-entry tile value is the same for every tile of the pass;
+        // the densify kernel adds each tile's column sums to the pass's
+        const bool reduced = p->precision != CREST_GRAM_FP64;
+        if (reduced && ds.scale) CREST_TRY(launch_tile_shift(p->w, ds, st));
+        // strictly gene-sorted rows (known once the range index exists) under a
+        // monotone column map give strictly increasing columns in every cell
+        const bool check_order = !(m->rows_strict && columns_monotone(gene_map, m->n_genes, sub_map, n_vars));
         int64_t u0 = 0;
         for (size_t u = 0; u < m->up_end.size() && u0 < m->n_cells; ++u) {
             const int64_t u1 = m->up_end[u];
@@ -779,12 +803,12 @@ int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
                 CREST_TRY(issue_uploads(m, u + 2));  // keep the next chunk's copy queued
                 CREST_CUDA_TRY(cudaStreamWaitEvent(st, m->up_ev[u], 0));
             }
-            CREST_TRY(compact_extract(m, proto, p->d, u0, u1, st));
+            CREST_TRY(compact_extract(m, proto, p->d, u0, u1, check_order, st));
             for (int64_t s0 = u0; s0 < u1; s0 += p->w.m_cap) {
                 const int64_t n = std::min(p->w.m_cap, u1 - s0);
-                CREST_TRY(
-                    launch_densify_compact(m->d_indptr.as<int64_t>(), s0, n, ch, target_sum, log1p, ds, p->w, st));
-                CREST_TRY(launch_syrk_fold(p->w, n, ds, p->gram.as<double>(), p->colsum.as<double>(), st));
+                CREST_TRY(launch_densify_compact(m->d_indptr.as<int64_t>(), s0, n, ch, target_sum, log1p, ds, p->w,
+                                                 st, reduced ? p->colsum.as<double>() : nullptr, true));
+                CREST_TRY(launch_syrk_fold(p->w, n, ds, p->gram.as<double>(), p->colsum.as<double>(), st, !reduced));
             }
             u0 = u1;
         }

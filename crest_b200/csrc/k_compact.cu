@@ -64,7 +64,7 @@ __device__ __forceinline__ int64_t gene_class_words_dev(int64_t n_gene_map) {
 template <int DEPTH>
 __global__ void __launch_bounds__(kExtractWarps * 32, 4) k_extract(DevChunk c, const uint32_t *__restrict__ cls,
                                                                 const int32_t *__restrict__ code, int32_t d,
-                                                                CompactHvg out) {
+                                                                int check_order, CompactHvg out) {
     extern __shared__ __align__(16) uint32_t s_cls[];
     const int64_t n16 = (int64_t)gene_class_words_dev(c.n_gene_map) / 4;
     for (int64_t j = threadIdx.x; j < n16; j += blockDim.x)
@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(kExtractWarps * 32, 4) k_extract(DevChunk c, c
             int cnt;
             int pos = nq + block_rank4(hv, cnt);
             if (cnt == 0) return;
-            order_check4(hv, col, carry, ordered);
+            if (check_order) order_check4(hv, col, carry, ordered);
 #pragma unroll
             for (int u = 0; u < 4; ++u)
                 if (hv[u]) {
@@ -144,10 +144,202 @@ __global__ void __launch_bounds__(kExtractWarps * 32, 4) k_extract(DevChunk c, c
     if (!__all_sync(kFull, ordered) && lane == 0) atomicOr(out.status, 1);
 }
 
+// ------------------------------------------------ extract, 16-bit codes
+// The same pass with the int16 code of every store gene in shared memory
+// (-1 dropped, d kept outside the HVG columns, else the HVG column), when
+// d < 32767 and the table leaves room for two blocks per SM: one
+// shared-memory load per entry gives both the class and the column.  Store
+// ids past the gene map are clamped onto one extra dropped slot, so the
+// full 128-entry blocks need no bounds checks; the loads of the next
+// DEPTH blocks are in flight while one is processed.  Whether
+// every kept value is a non-negative integer is tracked as the OR of the
+// bit patterns of x - rint(x) and of the sign bit of x (zero for exactly
+// those values).  The column-order check runs only when the rows are not
+// known to be strictly gene-sorted under a monotone column map.
+constexpr int kExtract16Warps = 8;
+
+__host__ __device__ inline int64_t code16_slots(int64_t n_gene_map) { return round_up(n_gene_map + 1, 8); }
+
+// The reference's entry-order f64 sum of a cell's kept values (the rare
+// path: some kept value is not a small non-negative integer); out of line so
+// that its registers do not weigh on the streaming loop.
+__device__ __noinline__ double kept_total_ordered16(const DevChunk &c, int64_t lo, int64_t hi, const int16_t *s_code) {
+    OrderedSum ts;
+    for_entries_by<4, false>(c, lo, hi, [&](uint32_t g) { return s_code[g] < 0 ? -1 : 0; },
+                             [&](int32_t m, float x) { ts.add(m != -1 ? (double)x : 0.0); });
+    return ts.acc;
+}
+
+template <int DEPTH>
+__global__ void __launch_bounds__(kExtract16Warps * 32, 3)
+    k_extract16(DevChunk c, const int16_t *__restrict__ code16, int32_t d, int check_order, CompactHvg out) {
+    extern __shared__ __align__(16) int16_t s_code[];
+    {
+        const int64_t n_words = code16_slots(c.n_gene_map) / 8, n_src = round_up(c.n_gene_map, 8) / 8;
+        for (int64_t j = threadIdx.x; j < n_words; j += blockDim.x)
+            reinterpret_cast<uint4 *>(s_code)[j] =
+                j < n_src ? __ldg(reinterpret_cast<const uint4 *>(code16) + j) : make_uint4(~0u, ~0u, ~0u, ~0u);
+    }
+    __syncthreads();
+    const int lane = lane_id();
+    const unsigned lt = (1u << lane) - 1u;
+    const uint32_t gclamp = (uint32_t)c.n_gene_map;  // a dropped slot
+    const int64_t warp = (int64_t)blockIdx.x * kExtract16Warps + (threadIdx.x >> 5);
+    const int64_t n_warps = (int64_t)gridDim.x * kExtract16Warps;
+    const bool norm = c.target_sum > 0.0;
+    const uintptr_t ga = reinterpret_cast<uintptr_t>(c.genes), va = reinterpret_cast<uintptr_t>(c.values);
+    const bool vec = ((ga ^ va) & 15) == 0;
+    bool ordered = true;
+    for (int64_t i = warp; i < c.n_spans; i += n_warps) {
+        int64_t lo, hi;
+        const int64_t row = span_row(c, i, lo, hi);
+        const int64_t cell = c.first_cell + i;
+        if (row < 0) {
+            if (lane == 0) out.n[cell] = -1;
+            continue;
+        }
+        int32_t *oc = out.code + lo;
+        float *ox = out.x + lo;
+        float fsum = 0.0f;  // kept values, exact while integral and below 2^24
+        uint32_t bad = 0u;  // nonzero once a kept value is not a non-negative integer
+        int nq = 0;
+        int32_t carry = -1;
+        // lane l holds entries 4l .. 4l + 3 of the block (padding: g = gclamp, x = 0)
+        auto block = [&](const uint32_t(&g)[4], const float(&x)[4]) {
+            int32_t v[4];
+            bool hv[4];
+            int before = 0, cnt = 0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                v[u] = s_code[min(g[u], gclamp)];
+                if (norm) {
+                    const float xk = v[u] >= 0 ? x[u] : 0.0f;
+                    fsum += xk;
+                    bad |= __float_as_uint(xk - rintf(xk)) | (__float_as_uint(xk) & 0x80000000u);
+                }
+                hv[u] = (uint32_t)v[u] < (uint32_t)d;
+                const unsigned bal = __ballot_sync(kFull, hv[u]);
+                before += __popc(bal & lt);
+                cnt += __popc(bal);
+            }
+            if (cnt == 0) return;  // warp-uniform
+            if (check_order) order_check4(hv, v, carry, ordered);
+            int pos = nq + before;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (hv[u]) {
+                    oc[pos] = v[u];
+                    ox[pos] = x[u];
+                    ++pos;
+                }
+            nq += cnt;
+        };
+        int64_t b = lo;
+        if (vec && lo < hi) {
+            // up to 3 entries before the first 16-byte boundary, one per lane
+            const int64_t head = (int64_t)((16 - ((ga + 4 * (uintptr_t)lo) & 15)) & 15) / 4;
+            if (head > 0) {
+                const int64_t hb = lo + head < hi ? lo + head : hi;
+                uint32_t g[4] = {gclamp, gclamp, gclamp, gclamp};
+                float x[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                if (lo + lane < hb) {
+                    g[0] = __ldcs(c.genes + lo + lane);
+                    x[0] = __ldcs(c.values + lo + lane);
+                }
+                block(g, x);
+                b = hb;
+            }
+            // whole blocks, DEPTH of them loading ahead
+            constexpr int NB = DEPTH + 1;
+            const int64_t nfull = (hi - b) / 128;
+            const uint4 *gp = reinterpret_cast<const uint4 *>(c.genes + b) + lane;
+            const float4 *xp = reinterpret_cast<const float4 *>(c.values + b) + lane;
+            uint4 gq[NB];
+            float4 xq[NB];
+#pragma unroll
+            for (int k = 0; k < NB; ++k)
+                if (k < nfull) {
+                    gq[k] = __ldcs(gp + 32 * k);
+                    xq[k] = __ldcs(xp + 32 * k);
+                }
+            for (int64_t t = 0; t < nfull; t += NB) {
+#pragma unroll
+                for (int k = 0; k < NB; ++k) {
+                    if (t + k >= nfull) break;  // warp-uniform
+                    const uint32_t g[4] = {gq[k].x, gq[k].y, gq[k].z, gq[k].w};
+                    const float x[4] = {xq[k].x, xq[k].y, xq[k].z, xq[k].w};
+                    if (t + k + NB < nfull) {
+                        gq[k] = __ldcs(gp + 32 * (t + k + NB));
+                        xq[k] = __ldcs(xp + 32 * (t + k + NB));
+                    }
+                    block(g, x);
+                }
+            }
+            b += nfull * 128;
+        }
+        // the partial last block (or every block when genes and values are
+        // not aligned alike), entry by entry
+        for (; b < hi; b += 128) {
+            uint32_t g[4];
+            float x[4];
+            const int64_t e = b + 4 * lane;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const bool ok = e + u < hi;
+                g[u] = ok ? __ldcs(c.genes + e + u) : gclamp;
+                x[u] = ok ? __ldcs(c.values + e + u) : 0.0f;
+            }
+            block(g, x);
+        }
+        double scale = 1.0;
+        if (norm) {
+            double total;
+            if (__all_sync(kFull, bad == 0u && fsum < 16777216.0f)) {
+                total = warp_sum((double)fsum);  // integers: every order gives the in-order f64 sum
+            } else {
+                total = kept_total_ordered16(c, lo, hi, s_code);
+            }
+            scale = total > 0.0 ? c.target_sum / total : 1.0;
+        }
+        if (lane == 0) {
+            out.n[cell] = nq;
+            out.scale[cell] = scale;
+        }
+    }
+    if (!__all_sync(kFull, ordered) && lane == 0) atomicOr(out.status, 1);
+}
+
 int launch_extract(const DevChunk &c, const uint32_t *cls, const int32_t *code, int64_t d, const CompactHvg &out,
-                   cudaStream_t st) {
+                   bool check_order, cudaStream_t st) {
     if (c.n_spans == 0) return CREST_OK;
     CREST_REQUIRE(!c.span_cell, CREST_EINVAL, "extract needs CSR chunks");
+    if (d < 32767) {  // the int16 codes exist (launch_hvg_code)
+        static const int depth = [] {  // blocks loading ahead (tuning; 1 or 2)
+            const char *e = getenv("CREST_EXTRACT_DEPTH");
+            return e && e[0] == '2' ? 2 : 1;
+        }();
+        const void *fn = depth == 2 ? (const void *)k_extract16<2> : (const void *)k_extract16<1>;
+        const size_t smem = 2 * (size_t)code16_slots(c.n_gene_map);
+        int per_sm = 0;
+        if (smem <= (size_t)kMaxSmem) {
+            CREST_TRY(ensure_smem_attr(fn, smem));
+            CREST_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kExtract16Warps * 32, smem));
+        }
+        if (per_sm >= 2) {
+            const int64_t blocks =
+                std::min<int64_t>(ceil_div(c.n_spans, kExtract16Warps), (int64_t)device_sms() * per_sm);
+            const int16_t *tab = codes16(code, c.n_gene_map);
+            prof::Scope ps("extract_csr", st);
+            if (depth == 2)
+                k_extract16<2><<<(unsigned)blocks, kExtract16Warps * 32, smem, st>>>(c, tab, (int32_t)d,
+                                                                                     check_order ? 1 : 0, out);
+            else
+                k_extract16<1><<<(unsigned)blocks, kExtract16Warps * 32, smem, st>>>(c, tab, (int32_t)d,
+                                                                                     check_order ? 1 : 0, out);
+            CREST_CUDA_TRY(cudaGetLastError());
+            return CREST_OK;
+        }
+    }
     const size_t smem = 4 * gene_class_words(c.n_gene_map);
     CREST_REQUIRE(smem <= (size_t)kMaxSmem, CREST_EINVAL, "too many genes for the class table");
     CREST_TRY(ensure_smem_attr((const void *)k_extract<1>, smem));
@@ -155,7 +347,8 @@ int launch_extract(const DevChunk &c, const uint32_t *cls, const int32_t *code, 
     CREST_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_extract<1>, kExtractWarps * 32, smem));
     const int64_t blocks = std::min<int64_t>(ceil_div(c.n_spans, kExtractWarps), (int64_t)device_sms() * std::max(per_sm, 1));
     prof::Scope ps("extract_csr", st);
-    k_extract<1><<<(unsigned)blocks, kExtractWarps * 32, smem, st>>>(c, cls, code, (int32_t)d, out);
+    k_extract<1><<<(unsigned)blocks, kExtractWarps * 32, smem, st>>>(c, cls, code, (int32_t)d, check_order ? 1 : 0,
+                                                                     out);
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
 }
@@ -216,8 +409,8 @@ template <> struct CElem<0> { using T = double; };
 template <> struct CElem<1> { using T = float; };
 template <> struct CElem<2> { using T = __nv_bfloat16; };
 
-template <int MODE>
-__global__ void __launch_bounds__(kDensifyCWarps * 32) k_densify_compact(
+template <int MODE, int MINB, int DU>
+__global__ void __launch_bounds__(kDensifyCWarps * 32, MINB) k_densify_compact(
     const int64_t *__restrict__ indptr, int64_t cell0, int64_t n_cells, CompactHvg in, double target_sum, int log1p,
     DevScale t, const double *__restrict__ shift, int64_t d, int64_t d_pad, int64_t m_pad, void *tile,
     double *__restrict__ colsum, long long *__restrict__ col_part, int64_t *n_kept) {
@@ -270,17 +463,17 @@ __global__ void __launch_bounds__(kDensifyCWarps * 32) k_densify_compact(
         E *row_lo = lo_plane + (size_t)i * d_pad;
         // the cell's entries in rounds of 32 x kDensifyU, every load of a
         // round issued before the first is used
-        for (int e0 = 0; e0 < n; e0 += 32 * kDensifyU) {
-            int32_t subs[kDensifyU];
-            float xs[kDensifyU];
+        for (int e0 = 0; e0 < n; e0 += 32 * DU) {
+            int32_t subs[DU];
+            float xs[DU];
 #pragma unroll
-            for (int u = 0; u < kDensifyU; ++u) {
+            for (int u = 0; u < DU; ++u) {
                 const int e = e0 + 32 * u + lane;
                 subs[u] = e < n ? __ldcs(in.code + base + e) : -1;
                 xs[u] = e < n ? __ldcs(in.x + base + e) : 0.0f;
             }
 #pragma unroll
-            for (int u = 0; u < kDensifyU; ++u) {
+            for (int u = 0; u < DU; ++u) {
             const int32_t sub = subs[u];
             if (sub < 0) continue;
             const double s = scale_value(t, sub, transform_value(tc, scale, xs[u]));
@@ -313,8 +506,10 @@ __global__ void __launch_bounds__(kDensifyCWarps * 32) k_densify_compact(
 }
 
 // colsum[j] += (sum over blocks of part[b][j]) 2^-32: an exact integer sum,
-// one warp per column (lanes over blocks).
-__global__ void k_colsum_reduce(const long long *__restrict__ part, int nb, int64_t d, double *__restrict__ colsum) {
+// one warp per column (lanes over blocks).  With `pass`, the tile's finished
+// column sum is also added there (the sum over the whole Gram pass).
+__global__ void k_colsum_reduce(const long long *__restrict__ part, int nb, int64_t d, double *__restrict__ colsum,
+                                double *__restrict__ pass) {
     const int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (j >= d) return;
@@ -322,37 +517,60 @@ __global__ void k_colsum_reduce(const long long *__restrict__ part, int nb, int6
     for (int b = lane; b < nb; b += 32) s += part[(int64_t)b * d + j];
 #pragma unroll
     for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    if (lane == 0 && s != 0) colsum[j] += (double)s * 0x1.0p-32;
+    if (lane == 0) {
+        const double v = colsum[j] + (double)s * 0x1.0p-32;
+        colsum[j] = v;
+        if (pass) pass[j] += v;
+    }
 }
 
-template <int MODE>
+// Resident blocks per SM and entry loads per lane in flight: two blocks of
+// 16 warps with eight loads each (64 registers), or three blocks with four
+// (40 registers; CREST_DENSIFY_OCC=3).
+template <int MODE, int MINB, int DU>
 static int densify_compact_t(const int64_t *indptr, int64_t cell0, int64_t n, const CompactHvg &in,
                              double target_sum, int log1p, const DevScale &t, const double *shift,
-                             const GramWork &w, int64_t m_pad, cudaStream_t st) {
+                             const GramWork &w, int64_t m_pad, cudaStream_t st, double *col_pass) {
     using E = typename CElem<MODE>::T;
+    const auto kern = k_densify_compact<MODE, MINB, DU>;
     const size_t smem = MODE != 0 ? sizeof(double) * (size_t)round_up(w.d, 2) + sizeof(E) * (size_t)w.d_pad : 0;
     CREST_REQUIRE(smem <= (size_t)kMaxSmem, CREST_EINVAL, "d=%lld too large for the densify buffers", (long long)w.d);
-    CREST_TRY(ensure_smem_attr((const void *)k_densify_compact<MODE>, smem));
+    CREST_TRY(ensure_smem_attr((const void *)kern, smem));
     int per_sm = 0;
-    CREST_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_densify_compact<MODE>,
-                                                                 kDensifyCWarps * 32, smem));
-    // at most two blocks per SM (the rows of the column-sum partials)
+    CREST_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kDensifyCWarps * 32, smem));
+    // the rows of the column-sum partials bound the block count
     const int64_t blocks = std::min<int64_t>(ceil_div(m_pad, kDensifyCWarps),
                                              std::min<int64_t>(w.colsum_rows, (int64_t)device_sms() * std::max(per_sm, 1)));
-    k_densify_compact<MODE><<<(unsigned)blocks, kDensifyCWarps * 32, smem, st>>>(
-        indptr, cell0, n, in, target_sum, log1p, t, shift, w.d, w.d_pad, m_pad, w.tile, w.colsum_chunk,
-        w.colsum_part, w.n_kept);
+    kern<<<(unsigned)blocks, kDensifyCWarps * 32, smem, st>>>(indptr, cell0, n, in, target_sum, log1p, t, shift, w.d,
+                                                              w.d_pad, m_pad, w.tile, w.colsum_chunk, w.colsum_part,
+                                                              w.n_kept);
     CREST_CUDA_TRY(cudaGetLastError());
     if (MODE != 0 && w.d > 0) {
         k_colsum_reduce<<<(unsigned)ceil_div(w.d * 32, 256), 256, 0, st>>>(w.colsum_part, (int)blocks, w.d,
-                                                                          w.colsum_chunk);
+                                                                          w.colsum_chunk, col_pass);
         CREST_CUDA_TRY(cudaGetLastError());
     }
     return CREST_OK;
 }
 
+template <int MODE>
+static int densify_compact_t(const int64_t *indptr, int64_t cell0, int64_t n, const CompactHvg &in,
+                             double target_sum, int log1p, const DevScale &t, const double *shift,
+                             const GramWork &w, int64_t m_pad, cudaStream_t st, double *col_pass) {
+    static const bool occ3 = [] {
+        const char *e = getenv("CREST_DENSIFY_OCC");
+        return e && e[0] == '3';
+    }();
+    if (occ3)
+        return densify_compact_t<MODE, 3, 4>(indptr, cell0, n, in, target_sum, log1p, t, shift, w, m_pad, st,
+                                             col_pass);
+    return densify_compact_t<MODE, 2, kDensifyU>(indptr, cell0, n, in, target_sum, log1p, t, shift, w, m_pad, st,
+                                                 col_pass);
+}
+
 int launch_densify_compact(const int64_t *indptr, int64_t cell0, int64_t n, const CompactHvg &in, double target_sum,
-                           int log1p, const DevScale &t, const GramWork &w, cudaStream_t st) {
+                           int log1p, const DevScale &t, const GramWork &w, cudaStream_t st, double *colsum_pass,
+                           bool shift_ready) {
     CREST_REQUIRE(n <= w.m_cap, CREST_EINVAL, "tile holds %lld cells, piece has %lld", (long long)w.m_cap,
                   (long long)n);
     const int64_t m_pad = round_up(n > 0 ? n : 1, 64);
@@ -360,15 +578,15 @@ int launch_densify_compact(const int64_t *indptr, int64_t cell0, int64_t n, cons
     CREST_CUDA_TRY(cudaMemsetAsync(w.colsum_chunk, 0, sizeof(double) * (size_t)(w.d > 0 ? w.d : 1), st));
     const double *shift = nullptr;
     if (w.precision != CREST_GRAM_FP64 && t.scale) {
-        CREST_TRY(launch_tile_shift(w, t, st));
+        if (!shift_ready) CREST_TRY(launch_tile_shift(w, t, st));  // the same for every tile of a pass
         shift = w.shift;
     }
     prof::Scope ps("densify", st);
     if (w.precision == CREST_GRAM_FP64)
-        return densify_compact_t<0>(indptr, cell0, n, in, target_sum, log1p, t, nullptr, w, m_pad, st);
+        return densify_compact_t<0>(indptr, cell0, n, in, target_sum, log1p, t, nullptr, w, m_pad, st, colsum_pass);
     if (w.precision == CREST_GRAM_FP32)
-        return densify_compact_t<1>(indptr, cell0, n, in, target_sum, log1p, t, shift, w, m_pad, st);
-    return densify_compact_t<2>(indptr, cell0, n, in, target_sum, log1p, t, shift, w, m_pad, st);
+        return densify_compact_t<1>(indptr, cell0, n, in, target_sum, log1p, t, shift, w, m_pad, st, colsum_pass);
+    return densify_compact_t<2>(indptr, cell0, n, in, target_sum, log1p, t, shift, w, m_pad, st, colsum_pass);
 }
 
 // ------------------------------------------------------------ project
@@ -460,6 +678,105 @@ __global__ void __launch_bounds__(kPCWarps * 32) k_project_compact(const int64_t
     }
 }
 
+// The same pass for an even k above 32: lane l owns the column pairs
+// (2l, 2l + 1) and (64 + 2l, 65 + 2l) (NP pairs), read as one 16-byte load
+// each, so an entry costs NP row loads instead of 2 NP; the staged columns
+// and values of 8 entries are read from shared memory as vectors.  Every
+// column still sees the same f64 multiplies and additions in entry order.
+template <int NP>
+__global__ void __launch_bounds__(kPCWarps * 32) k_project_pairs(const int64_t *__restrict__ indptr,
+                                                                 int64_t n_cells, const int64_t *__restrict__ cell_map,
+                                                                 CompactHvg in, double target_sum, int log1p,
+                                                                 DevScale t, const double *__restrict__ V, int k,
+                                                                 float *__restrict__ out) {
+    constexpr int U = 8, WARPS = kPCWarps, STAGE = kPCStage;
+    __shared__ __align__(16) double s_val[WARPS][STAGE];
+    __shared__ __align__(16) int32_t s_code[WARPS][STAGE];
+    const int lane = lane_id(), wid = threadIdx.x >> 5;
+    double *q_val = s_val[wid];
+    int32_t *q_code = s_code[wid];
+    const int64_t warp = (int64_t)blockIdx.x * WARPS + wid;
+    const int64_t n_warps = (int64_t)gridDim.x * WARPS;
+    bool ok[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) ok[p] = 64 * p + 2 * lane < k;
+    DevChunk tc;
+    tc.target_sum = target_sum;
+    tc.log1p = log1p;
+    for (int64_t i = warp; i < n_cells; i += n_warps) {
+        const int n = in.n[i];
+        if (n < 0) continue;
+        const int64_t row = cell_map[i];
+        const double scale = in.scale[i];
+        const int64_t base = indptr[i];
+        double2 acc[NP];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) acc[p] = make_double2(0.0, 0.0);
+        auto add = [&](double sv, const double2 &v, double2 &a) {
+            a.x = __dadd_rn(a.x, __dmul_rn(sv, v.x));
+            a.y = __dadd_rn(a.y, __dmul_rn(sv, v.y));
+        };
+        for (int r0 = 0; r0 < n; r0 += STAGE) {
+            const int m = n - r0 < STAGE ? n - r0 : STAGE;
+            __syncwarp();
+            for (int e = lane; e < m; e += 32) {
+                const int32_t sub = __ldcs(in.code + base + r0 + e);
+                q_code[e] = sub;
+                q_val[e] = scale_value(t, sub, transform_value(tc, scale, __ldcs(in.x + base + r0 + e)));
+            }
+            __syncwarp();
+            int e = 0;
+            for (; e + U <= m; e += U) {
+                const int4 c0 = *reinterpret_cast<const int4 *>(q_code + e);
+                const int4 c1 = *reinterpret_cast<const int4 *>(q_code + e + 4);
+                const int32_t cc[U] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+                double2 vv[U][NP];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const double2 *vr = reinterpret_cast<const double2 *>(V + (size_t)cc[u] * k) + lane;
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) vv[u][p] = ok[p] ? __ldg(vr + 32 * p) : make_double2(0.0, 0.0);
+                }
+#pragma unroll
+                for (int u = 0; u < U; u += 2) {
+                    const double2 sv = *reinterpret_cast<const double2 *>(q_val + e + u);
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) add(sv.x, vv[u][p], acc[p]);
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) add(sv.y, vv[u + 1][p], acc[p]);
+                }
+            }
+            for (; e < m; ++e) {
+                const double2 *vr = reinterpret_cast<const double2 *>(V + (size_t)q_code[e] * k) + lane;
+                const double sv = q_val[e];
+#pragma unroll
+                for (int p = 0; p < NP; ++p)
+                    if (ok[p]) add(sv, __ldg(vr + 32 * p), acc[p]);
+            }
+        }
+        float *o = out + (size_t)row * k;
+#pragma unroll
+        for (int p = 0; p < NP; ++p)
+            if (ok[p]) {
+                const int j = 64 * p + 2 * lane;
+                atomicAdd(o + j, __double2float_rn(acc[p].x));
+                atomicAdd(o + j + 1, __double2float_rn(acc[p].y));
+            }
+    }
+}
+
+template <class K>
+static int project_launch(K kern, const int64_t *indptr, int64_t n_cells, const int64_t *cell_map,
+                          const CompactHvg &in, double target_sum, int log1p, const DevScale &t, const double *V, int k,
+                          float *out, cudaStream_t st) {
+    int per_sm = 0;
+    CREST_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPCWarps * 32, 0));
+    const int64_t blocks = std::min<int64_t>(ceil_div(n_cells, kPCWarps), (int64_t)device_sms() * std::max(per_sm, 1));
+    kern<<<(unsigned)blocks, kPCWarps * 32, 0, st>>>(indptr, n_cells, cell_map, in, target_sum, log1p, t, V, k, out);
+    CREST_CUDA_TRY(cudaGetLastError());
+    return CREST_OK;
+}
+
 template <int KPL>
 static int project_compact_k(const int64_t *indptr, int64_t n_cells, const int64_t *cell_map, const CompactHvg &in,
                              double target_sum, int log1p, const DevScale &t, const double *V, int k, float *out,
@@ -480,6 +797,10 @@ int launch_project_compact(const int64_t *indptr, int64_t n_cells, const int64_t
     CREST_REQUIRE(k <= 128, CREST_EINVAL, "project supports k <= 128 (got %d)", k);
     (void)d;
     prof::Scope ps("project_compact", st);
+    const bool pairs = k > 32 && k % 2 == 0 && (reinterpret_cast<uintptr_t>(V) & 15) == 0;
+    if (pairs && k <= 64)
+        return project_launch(k_project_pairs<1>, indptr, n_cells, cell_map, in, target_sum, log1p, t, V, k, out, st);
+    if (pairs) return project_launch(k_project_pairs<2>, indptr, n_cells, cell_map, in, target_sum, log1p, t, V, k, out, st);
     if (k <= 32) return project_compact_k<1>(indptr, n_cells, cell_map, in, target_sum, log1p, t, V, k, out, st);
     if (k <= 64) return project_compact_k<2>(indptr, n_cells, cell_map, in, target_sum, log1p, t, V, k, out, st);
     return project_compact_k<4>(indptr, n_cells, cell_map, in, target_sum, log1p, t, V, k, out, st);

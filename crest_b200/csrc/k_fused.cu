@@ -20,9 +20,12 @@
 //   dL/dx_e  = dL/dy_e / sf_c
 //   dL/dsf_c = - sum_e dL/dy_e y_e / sf_c
 //   dL/dW[g, :] = sum over entries of gene g of s_e G[c_e, :]
-// log1p and the scaled values are recomputed in the backward pass; only the
-// per-entry s_e of the stored entries is kept for the W gradient, which is
-// formed gene by gene over a by-gene index of the entries (counting sort).
+// log1p and the scaled values are recomputed in the backward pass.  The W
+// gradient is formed gene by gene: a per-gene histogram of the entries and
+// its scan give every gene a segment, the entry pass writes (s_e, c_e) of
+// each entry into its gene's segment (counting sort; the order inside a
+// segment is not fixed), and one block per gene sums s_e G[c_e, :] over its
+// segment in f64.
 #include "host.cuh"
 #include "prof.cuh"
 #include "rowwarp.cuh"
@@ -55,6 +58,11 @@ __device__ __forceinline__ double fused_value(const FusedArgs &a, int32_t g, flo
     return __dsub_rn(clip_mv(z, mv), clip_mv(__ddiv_rn(-mu, sd), mv));
 }
 
+// Warp per cell; lane j of the warp owns score columns j, j + 32, ...  Each
+// 32-entry segment is transformed lane-parallel, then folded into the
+// scores in entry order.  (Loading the W rows of 8 entries ahead of their
+// additions needs 80 registers and measured slower, 0.84 against 0.61 ms on
+// the 50,000-cell workload: the occupancy it costs hides more latency.)
 template <int KPL>
 __global__ void __launch_bounds__(256) k_fused_fwd(FusedArgs a, float *__restrict__ scores) {
     const int lane = threadIdx.x & 31;
@@ -101,54 +109,35 @@ __global__ void __launch_bounds__(256) k_fused_fwd(FusedArgs a, float *__restric
     }
 }
 
-// Entry pass of the backward: dL/dx, dL/dsf, and s_e / cell of every entry
-// for the W gradient; per-gene entry counts for the by-gene index.
-template <int KPL>
-__global__ void __launch_bounds__(256) k_fused_bwd_entries(FusedArgs a, const float *__restrict__ G,
-                                                           float *__restrict__ grad_x, float *__restrict__ grad_sf,
-                                                           double *__restrict__ s_out, int32_t *__restrict__ cell_out,
-                                                           int32_t *__restrict__ gene_count) {
-    __shared__ float g_row[8][32 * KPL];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t c = warp; c < a.n; c += n_warps) {
-        __syncwarp();
-#pragma unroll
-        for (int q = 0; q < KPL; ++q) {
-            const int j = lane + 32 * q;
-            g_row[wid][j] = j < a.k ? G[c * a.k + j] : 0.0f;
-        }
-        __syncwarp();
-        const int64_t lo = a.indptr[c], hi = a.indptr[c + 1];
-        const float sfc = a.sf[c];
-        double dsf = 0.0;
-        for (int64_t e = lo + lane; e < hi; e += 32) {
-            const int32_t g = __ldg(a.indices + e);
-            if (g < 0 || g >= a.d) {  // out-of-range gene id: reported, no gradient
-                *a.bad = 1;
-                grad_x[e] = 0.0f;
-                s_out[e] = 0.0;
-                cell_out[e] = (int32_t)c;
-                continue;
-            }
-            const float x = __ldg(a.values + e);
-            float y;
-            double pass;
-            const double s = fused_value(a, g, x, sfc, y, pass);
-            const float *wr = a.W + (size_t)g * a.k;
-            double gs = 0.0;
-            for (int j = 0; j < a.k; ++j) gs = fma((double)g_row[wid][j], (double)__ldg(wr + j), gs);
-            const double dy = gs * pass / (__ldg(a.std + g) * (1.0 + (double)y));
-            grad_x[e] = (float)(dy / (double)sfc);
-            dsf -= dy * (double)y / (double)sfc;
-            s_out[e] = s;
-            cell_out[e] = (int32_t)c;
-            atomicAdd(gene_count + g, 1);
-        }
-        dsf = warp_sum(dsf);
-        if (lane == 0) grad_sf[c] = (float)dsf;
+// The W gradient loads the G rows of kGather entries before their products.
+constexpr int kGather = 8;
+
+// Per-gene entry counts: block-private counters in shared memory when d
+// fits (kHistSmem genes), else global atomics; ids outside [0, d) are left
+// out (the entry pass reports them).
+constexpr int kHistSmem = 12288;
+
+__global__ void __launch_bounds__(256) k_gene_hist(const int32_t *__restrict__ indices, int64_t nnz, int64_t d,
+                                                   int32_t *__restrict__ count) {
+    __shared__ int32_t s_cnt[kHistSmem];
+    const bool priv = d <= kHistSmem;
+    if (priv)
+        for (int64_t g = threadIdx.x; g < d; g += blockDim.x) s_cnt[g] = 0;
+    __syncthreads();
+    const int64_t per = ceil_div(nnz, (int64_t)gridDim.x);
+    const int64_t e0 = per * blockIdx.x, e1 = e0 + per < nnz ? e0 + per : nnz;
+    for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const int32_t g = __ldg(indices + e);
+        if (g < 0 || g >= d) continue;
+        if (priv)
+            atomicAdd(s_cnt + g, 1);
+        else
+            atomicAdd(count + g, 1);
     }
+    __syncthreads();
+    if (priv)
+        for (int64_t g = threadIdx.x; g < d; g += blockDim.x)
+            if (s_cnt[g]) atomicAdd(count + g, s_cnt[g]);
 }
 
 // Exclusive scan of the per-gene counts (one block): offsets[0..d].
@@ -177,51 +166,143 @@ __global__ void __launch_bounds__(1024) k_scan_counts(const int32_t *count, int6
     }
 }
 
-__global__ void k_scatter_by_gene(const int32_t *__restrict__ indices, int64_t nnz, int64_t d,
-                                  const int64_t *__restrict__ offsets,
-                                  int32_t *__restrict__ fill, int64_t *__restrict__ order) {
-    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= nnz) return;
-    const int32_t g = indices[e];
-    if (g < 0 || g >= d) return;
-    order[offsets[g] + atomicAdd(fill + g, 1)] = e;
+// W rows padded to kp = round_up(k, 4) floats (16-byte rows for vector loads).
+__global__ void k_pad_rows(const float *__restrict__ W, int64_t d, int k, int kp, float *__restrict__ Wp) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= d * kp) return;
+    const int64_t g = i / kp;
+    const int j = (int)(i - g * kp);
+    Wp[i] = j < k ? W[g * k + j] : 0.0f;
 }
 
-// dL/dW[g, :] = sum over entries of gene g of s_e G[c_e, :], warp per gene.
-template <int KPL>
-__global__ void __launch_bounds__(256) k_fused_bwd_w(int64_t d, int k, const int64_t *__restrict__ offsets,
-                                                     const int64_t *__restrict__ order, const double *__restrict__ s_e,
-                                                     const int32_t *__restrict__ cell, const float *__restrict__ G,
-                                                     float *__restrict__ grad_W) {
-    const int lane = threadIdx.x & 31;
+// One entry's contribution to the W gradient: s_e and its cell.
+struct __align__(16) EntryCell {
+    double s;
+    int32_t cell;
+    int32_t pad;
+};
+
+// Entry pass of the backward, warp per cell, lane per entry: dL/dx and
+// dL/dsf, and (s_e, c) of every entry into its gene's segment.  The cell's
+// row of G is held in shared memory as f64 (kp columns, zero-padded); the
+// dot product with W[g, :] reads the W rows padded to kp (<= KP) columns,
+// 16 bytes at a time.
+template <int KP>
+__global__ void __launch_bounds__(256) k_fused_bwd_entries(FusedArgs a, const float *__restrict__ G,
+                                                           const float *__restrict__ Wp, int kp,
+                                                           float *__restrict__ grad_x, float *__restrict__ grad_sf,
+                                                           const int64_t *__restrict__ offsets,
+                                                           int32_t *__restrict__ fill, EntryCell *__restrict__ by_gene) {
+    __shared__ double g_row[8][KP];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t g = warp; g < d; g += n_warps) {
+    for (int64_t c = warp; c < a.n; c += n_warps) {
+        __syncwarp();
+        for (int j = lane; j < KP; j += 32) g_row[wid][j] = j < a.k ? (double)G[c * a.k + j] : 0.0;
+        __syncwarp();
+        const int64_t lo = a.indptr[c], hi = a.indptr[c + 1];
+        const float sfc = a.sf[c];
+        double dsf = 0.0;
+        for (int64_t e = lo + lane; e < hi; e += 32) {
+            const int32_t g = __ldg(a.indices + e);
+            if (g < 0 || g >= a.d) {  // out-of-range gene id: reported, no gradient
+                *a.bad = 1;
+                grad_x[e] = 0.0f;
+                continue;
+            }
+            const float x = __ldg(a.values + e);
+            float y;
+            double pass;
+            const double s = fused_value(a, g, x, sfc, y, pass);
+            const float4 *wr = reinterpret_cast<const float4 *>(Wp + (size_t)g * kp);
+            double gs = 0.0;
+#pragma unroll 4
+            for (int j4 = 0; j4 < kp / 4; ++j4) {
+                const float4 w = __ldg(wr + j4);
+                const double *gr = g_row[wid] + 4 * j4;
+                gs = fma(gr[0], (double)w.x, gs);
+                gs = fma(gr[1], (double)w.y, gs);
+                gs = fma(gr[2], (double)w.z, gs);
+                gs = fma(gr[3], (double)w.w, gs);
+            }
+            const double dy = gs * pass / (__ldg(a.std + g) * (1.0 + (double)y));
+            grad_x[e] = (float)(dy / (double)sfc);
+            dsf -= dy * (double)y / (double)sfc;
+            EntryCell ec;
+            ec.s = s;
+            ec.cell = (int32_t)c;
+            ec.pad = 0;
+            by_gene[offsets[g] + atomicAdd(fill + g, 1)] = ec;
+        }
+        dsf = warp_sum(dsf);
+        if (lane == 0) grad_sf[c] = (float)dsf;
+    }
+}
+
+// dL/dW[g, :] = sum over gene g's segment of s_e G[c_e, :], block per gene:
+// the 8 warps take interleaved 32-entry pieces of the segment (one
+// coalesced load of 32 (s, c) pairs per piece), lane j accumulates columns
+// j, j + 32, ...; the G rows of kGather entries are loaded before their
+// products are added.  The warps' partial sums are added in shared memory.
+template <int KPL>
+__global__ void __launch_bounds__(256) k_fused_bwd_w(int64_t d, int k, const int64_t *__restrict__ offsets,
+                                                     const EntryCell *__restrict__ by_gene,
+                                                     const float *__restrict__ G, float *__restrict__ grad_W) {
+    __shared__ double part[8][32 * KPL];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int64_t g = blockIdx.x; g < d; g += gridDim.x) {
+        const int64_t t0 = offsets[g], t1 = offsets[g + 1];
         double acc[KPL];
 #pragma unroll
         for (int q = 0; q < KPL; ++q) acc[q] = 0.0;
-        for (int64_t t = offsets[g]; t < offsets[g + 1]; ++t) {
-            const int64_t e = order[t];
-            const double s = s_e[e];
-            const float *gr = G + (size_t)cell[e] * k;
+        for (int64_t b = t0 + 32 * wid; b < t1; b += 256) {
+            const int cnt = t1 - b < 32 ? (int)(t1 - b) : 32;
+            double s = 0.0;
+            int32_t cell = 0;
+            if (lane < cnt) {
+                const EntryCell ec = by_gene[b + lane];
+                s = ec.s;
+                cell = ec.cell;
+            }
+            for (int u0 = 0; u0 < cnt; u0 += kGather) {
+                float gv[kGather][KPL];
+                double su[kGather];
 #pragma unroll
-            for (int q = 0; q < KPL; ++q) {
-                const int j = lane + 32 * q;
-                if (j < k) acc[q] = fma(s, (double)__ldg(gr + j), acc[q]);
+                for (int t = 0; t < kGather; ++t) {
+                    const int u = (u0 + t) & 31;
+                    su[t] = __shfl_sync(kFull, s, u);
+                    const int32_t cu = __shfl_sync(kFull, cell, u);
+                    const float *gr = G + (size_t)cu * k;
+#pragma unroll
+                    for (int q = 0; q < KPL; ++q) {
+                        const int j = lane + 32 * q;
+                        gv[t][q] = (u0 + t < cnt && j < k) ? __ldg(gr + j) : 0.0f;
+                    }
+                }
+#pragma unroll
+                for (int t = 0; t < kGather; ++t)
+#pragma unroll
+                    for (int q = 0; q < KPL; ++q) acc[q] = fma(su[t], (double)gv[t][q], acc[q]);
             }
         }
 #pragma unroll
-        for (int q = 0; q < KPL; ++q) {
-            const int j = lane + 32 * q;
-            if (j < k) grad_W[g * k + j] = (float)acc[q];
+        for (int q = 0; q < KPL; ++q) part[wid][lane + 32 * q] = acc[q];
+        __syncthreads();
+        for (int j = threadIdx.x; j < k; j += blockDim.x) {
+            double v = 0.0;
+#pragma unroll
+            for (int w = 0; w < 8; ++w) v += part[w][j];
+            grad_W[g * k + j] = (float)v;
         }
+        __syncthreads();
     }
 }
 
 int grid_warps(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, 8), device_sms() * 16)); }
 
 struct FusedWork {
-    DevBuf s, cell, count, fill, offsets, order, bad;
+    DevBuf by_gene, count, fill, offsets, wpad, bad;
 };
 
 FusedWork &fused_work(int dev) {
@@ -310,46 +391,52 @@ extern "C" int crest_fused_backward(const int64_t *indptr, const int32_t *indice
     }
     CREST_REQUIRE(p0 == 0 && nnz >= 0 && nnz < ((int64_t)1 << 31), CREST_EINVAL,
                   "fused map: indptr must start at 0 and hold < 2^31 entries");
-    CREST_TRY(w.s.ensure(sizeof(double) * (size_t)std::max<int64_t>(nnz, 1)));
-    CREST_TRY(w.cell.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1)));
-    CREST_TRY(w.order.ensure(sizeof(int64_t) * (size_t)std::max<int64_t>(nnz, 1)));
+    const int kp = (int)round_up(k, 4);
+    CREST_TRY(w.by_gene.ensure(sizeof(EntryCell) * (size_t)std::max<int64_t>(nnz, 1)));
     CREST_TRY(w.count.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(d, 1)));
     CREST_TRY(w.fill.ensure(sizeof(int32_t) * (size_t)std::max<int64_t>(d, 1)));
     CREST_TRY(w.offsets.ensure(sizeof(int64_t) * (size_t)(d + 1)));
+    CREST_TRY(w.wpad.ensure(sizeof(float) * (size_t)std::max<int64_t>(d * kp, 1)));
     if (d) {
         CREST_CUDA_TRY(cudaMemsetAsync(w.count.ptr, 0, sizeof(int32_t) * d, st));
         CREST_CUDA_TRY(cudaMemsetAsync(w.fill.ptr, 0, sizeof(int32_t) * d, st));
     }
-    if (n > 0) {
+    {
         prof::Scope ps("fused_bwd", st);
-        const int g = grid_warps(n);
-        if (k <= 32)
-            k_fused_bwd_entries<1><<<g, 256, 0, st>>>(a, grad_scores, grad_values, grad_sf, w.s.as<double>(),
-                                                      w.cell.as<int32_t>(), w.count.as<int32_t>());
-        else if (k <= 64)
-            k_fused_bwd_entries<2><<<g, 256, 0, st>>>(a, grad_scores, grad_values, grad_sf, w.s.as<double>(),
-                                                      w.cell.as<int32_t>(), w.count.as<int32_t>());
-        else
-            k_fused_bwd_entries<4><<<g, 256, 0, st>>>(a, grad_scores, grad_values, grad_sf, w.s.as<double>(),
-                                                      w.cell.as<int32_t>(), w.count.as<int32_t>());
+        if (d > 0) {
+            if (nnz)
+                k_gene_hist<<<(unsigned)std::min<int64_t>(ceil_div(nnz, 4096), device_sms() * 4), 256, 0, st>>>(
+                    indices, nnz, d, w.count.as<int32_t>());
+            k_scan_counts<<<1, 1024, 0, st>>>(w.count.as<int32_t>(), d, w.offsets.as<int64_t>());
+            k_pad_rows<<<(unsigned)ceil_div(d * kp, 256), 256, 0, st>>>(W, d, (int)k, kp, w.wpad.as<float>());
+        }
+        if (n > 0) {
+            const int g = grid_warps(n);
+            auto entries = [&](auto kern) {
+                kern<<<g, 256, 0, st>>>(a, grad_scores, w.wpad.as<float>(), kp, grad_values, grad_sf,
+                                        w.offsets.as<int64_t>(), w.fill.as<int32_t>(), w.by_gene.as<EntryCell>());
+            };
+            if (kp <= 32)
+                entries(k_fused_bwd_entries<32>);
+            else if (kp <= 64)
+                entries(k_fused_bwd_entries<64>);
+            else
+                entries(k_fused_bwd_entries<128>);
+        }
         CREST_CUDA_TRY(cudaGetLastError());
     }
     if (d > 0) {
         prof::Scope ps("fused_bwd_w", st);
-        k_scan_counts<<<1, 1024, 0, st>>>(w.count.as<int32_t>(), d, w.offsets.as<int64_t>());
-        if (nnz)
-            k_scatter_by_gene<<<(unsigned)ceil_div(nnz, 256), 256, 0, st>>>(indices, nnz, d, w.offsets.as<int64_t>(),
-                                                                          w.fill.as<int32_t>(), w.order.as<int64_t>());
-        const int g = grid_warps(d);
+        const unsigned blocks = (unsigned)std::min<int64_t>(d, (int64_t)device_sms() * 8);
         if (k <= 32)
-            k_fused_bwd_w<1><<<g, 256, 0, st>>>(d, (int)k, w.offsets.as<int64_t>(), w.order.as<int64_t>(),
-                                                w.s.as<double>(), w.cell.as<int32_t>(), grad_scores, grad_W);
+            k_fused_bwd_w<1><<<blocks, 256, 0, st>>>(d, (int)k, w.offsets.as<int64_t>(), w.by_gene.as<EntryCell>(),
+                                                     grad_scores, grad_W);
         else if (k <= 64)
-            k_fused_bwd_w<2><<<g, 256, 0, st>>>(d, (int)k, w.offsets.as<int64_t>(), w.order.as<int64_t>(),
-                                                w.s.as<double>(), w.cell.as<int32_t>(), grad_scores, grad_W);
+            k_fused_bwd_w<2><<<blocks, 256, 0, st>>>(d, (int)k, w.offsets.as<int64_t>(), w.by_gene.as<EntryCell>(),
+                                                     grad_scores, grad_W);
         else
-            k_fused_bwd_w<4><<<g, 256, 0, st>>>(d, (int)k, w.offsets.as<int64_t>(), w.order.as<int64_t>(),
-                                                w.s.as<double>(), w.cell.as<int32_t>(), grad_scores, grad_W);
+            k_fused_bwd_w<4><<<blocks, 256, 0, st>>>(d, (int)k, w.offsets.as<int64_t>(), w.by_gene.as<EntryCell>(),
+                                                     grad_scores, grad_W);
         CREST_CUDA_TRY(cudaGetLastError());
     }
     return bad_ids(w, st);

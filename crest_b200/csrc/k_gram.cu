@@ -514,7 +514,7 @@ __global__ void k_add_colsum(const double *__restrict__ src, int64_t d, double *
 }
 
 int launch_syrk_fold(const GramWork &w, int64_t m, const DevScale &t, double *gram, double *colsum,
-                     cudaStream_t st) {
+                     cudaStream_t st, bool add_colsum) {
     if (w.d == 0) return CREST_OK;
     const int64_t m_pad = round_up(m > 0 ? m : 1, 64);
     if (w.precision == CREST_GRAM_FP64) {
@@ -541,8 +541,10 @@ int launch_syrk_fold(const GramWork &w, int64_t m, const DevScale &t, double *gr
     } else {
         CREST_TRY(syrk_bf16x3_fold(w, m_pad, t, gram, st));
     }
-    k_add_colsum<<<(unsigned)ceil_div(w.d, 256), 256, 0, st>>>(w.colsum_chunk, w.d, colsum);
-    CREST_CUDA_TRY(cudaGetLastError());
+    if (add_colsum) {
+        k_add_colsum<<<(unsigned)ceil_div(w.d, 256), 256, 0, st>>>(w.colsum_chunk, w.d, colsum);
+        CREST_CUDA_TRY(cudaGetLastError());
+    }
     return CREST_OK;
 }
 

@@ -30,7 +30,8 @@ namespace crest {
 // Warp per cell.  Entry e's range is min(g >> log2_s, R-1); where the range
 // grows from the previous entry's (0 before the first entry) the
 // boundaries in between start at e.  Boundaries past the last entry start
-// at the row's end.  A descending gene id anywhere in a row sets *unsorted.
+// at the row's end.  A descending gene id anywhere in a row sets bit 0 of
+// *unsorted, a gene id equal to its predecessor's (a duplicate entry) bit 1.
 __global__ void __launch_bounds__(256) k_range_index(const int64_t *__restrict__ indptr,
                                                      const uint32_t *__restrict__ genes, int64_t n_cells,
                                                      int log2_s, int n_ranges, int32_t *__restrict__ off,
@@ -44,7 +45,7 @@ __global__ void __launch_bounds__(256) k_range_index(const int64_t *__restrict__
         int32_t *o = off + cell * nb;
         uint32_t carry_g = 0;  // gene of the previous entry
         int carry_r = 0;       // its range (0 before the first entry)
-        bool have_prev = false, bad = false;
+        bool have_prev = false, bad = false, dup = false;
         constexpr int U = 8;
         for (int64_t s = lo; s < hi; s += 32 * U) {
             uint32_t g[U];
@@ -65,7 +66,10 @@ __global__ void __launch_bounds__(256) k_range_index(const int64_t *__restrict__
                 const uint32_t prev_g = lane == 0 ? carry_g : gp;
                 const int prev_r = lane == 0 ? carry_r : rp_up;
                 const bool has_prev = lane == 0 ? have_prev : true;
-                if (valid && has_prev && g[u] < prev_g) bad = true;
+                if (valid && has_prev && g[u] <= prev_g) {
+                    bad = bad || g[u] < prev_g;
+                    dup = dup || g[u] == prev_g;
+                }
                 if (valid)
                     for (int b = prev_r + 1; b <= r; ++b) o[b - 1] = (int32_t)(e - lo);
                 const int last = hi - 1 - base < 31 ? (int)(hi - 1 - base) : 31;
@@ -75,7 +79,8 @@ __global__ void __launch_bounds__(256) k_range_index(const int64_t *__restrict__
             }
         }
         for (int b = carry_r + 1 + lane; b <= nb; b += 32) o[b - 1] = (int32_t)(hi - lo);
-        if (__any_sync(kFull, bad) && lane == 0) atomicOr(unsorted, 1);
+        const bool any_bad = __any_sync(kFull, bad), any_dup = __any_sync(kFull, dup);
+        if ((any_bad || any_dup) && lane == 0) atomicOr(unsorted, (any_bad ? 1 : 0) | (any_dup ? 2 : 0));
     }
 }
 

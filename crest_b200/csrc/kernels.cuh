@@ -56,7 +56,8 @@ struct RangeIndex {
     const int32_t *off;
 };
 constexpr int kSweepThreads = 768;
-// Builds the index; sets *unsorted to 1 if some row is not sorted.
+// Builds the index; ORs into *unsorted bit 0 if some row is not sorted by
+// gene, bit 1 if some row holds a gene id twice in a row.
 int launch_range_index(const int64_t *indptr, const uint32_t *genes, int64_t n_cells, int log2_s, int n_ranges,
                        int32_t *off, int *unsorted, cudaStream_t st);
 // Per-gene QC sums and per-row (t, n, f) of a piece whose spans are matrix
@@ -135,7 +136,7 @@ int launch_densify(const DevChunk &c, const int32_t *code, const DevScale &t, co
 // gram (d x d row-major, upper triangle) += T T^T of the current tile; adds
 // colsum_chunk to colsum.
 int launch_syrk_fold(const GramWork &w, int64_t m, const DevScale &t, double *gram, double *colsum,
-                     cudaStream_t st);
+                     cudaStream_t st, bool add_colsum = true);
 // Non-zero error word of the tensor-core Gram pipeline -> CREST_ETIMEOUT (and cleared).
 int tc_check_error();
 // gram += gram_aux, gram_aux = 0: once at the end of every Gram pass.
@@ -158,13 +159,19 @@ struct CompactHvg {
 size_t gene_class_words(int64_t n_gene_map);
 int launch_gene_class(const int32_t *code, int64_t n_gene_map, int64_t d, uint32_t *cls, cudaStream_t st);
 // One read of a whole CSR matrix (c.base == 0, CSR spans) into the compact form.
+// check_order = false when every row is known to be strictly gene-sorted and
+// the HVG columns increase with the gene id (the columns of every cell are
+// then strictly increasing and need no check).
 int launch_extract(const DevChunk &c, const uint32_t *cls, const int32_t *code, int64_t d, const CompactHvg &out,
-                   cudaStream_t st);
+                   bool check_order, cudaStream_t st);
 // Exact duplicate-column check of every cell (sets bit 1 of *in.status).
 int launch_dup_compact(const int64_t *indptr, int64_t n_cells, const CompactHvg &in, int64_t d, cudaStream_t st);
 // Densify cells [cell0, cell0 + n) of the compact form into the Gram tile.
+// colsum_pass: also add the tile's column sums there (reduced precisions);
+// shift_ready: launch_tile_shift already ran for this pass.
 int launch_densify_compact(const int64_t *indptr, int64_t cell0, int64_t n, const CompactHvg &in, double target_sum,
-                           int log1p, const DevScale &t, const GramWork &w, cudaStream_t st);
+                           int log1p, const DevScale &t, const GramWork &w, cudaStream_t st,
+                           double *colsum_pass = nullptr, bool shift_ready = false);
 // Streamed matrices: the HVG entries of chunk c (extracted into `scratch`,
 // slots as in the chunk buffer) packed into `packed` at running offsets
 // off[cell]; *total is the running entry count (bit 3 of *packed.status when

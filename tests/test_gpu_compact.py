@@ -64,7 +64,7 @@ def test_plan_fp64_gram_bit_exact(small_counts, residency):
     dm.close()
 
 
-@pytest.mark.parametrize("k", [20, 50])
+@pytest.mark.parametrize("k", [20, 50, 51, 100])
 def test_compact_projection_equals_csr_projection(small_counts, k):
     """The same plan (same loadings) projects a device-resident matrix from the
     compact form and a streamed one from the CSR: identical scores."""
@@ -94,6 +94,91 @@ def test_compact_projection_equals_csr_projection(small_counts, k):
     assert np.array_equal(Xz, Xo)
     for x in (p, dm, dh):
         x.close()
+
+
+def oracle_gram(s, indices=None, data=None, indptr=None):
+    Go, co = np.zeros((s["d"], s["d"])), np.zeros(s["d"])
+    oracle.gram_accumulate(s["indices"] if indices is None else indices, s["data"] if data is None else data,
+                           s["cm"], s["gm"], 1e4, True, None, s["indptr"] if indptr is None else indptr, 0, s["sub"],
+                           Go, co, True, s["mean"], s["std"], 10.0)
+    return Go, co
+
+
+def build_range_index(s, dm):
+    """A QC pass over a device matrix builds its gene-range index, which also
+    records whether every row is strictly sorted by gene."""
+    nr, nv = s["nr"], s["nv"]
+    flag = np.zeros(nv, np.bool_)
+    out = [np.zeros(nr), np.zeros(nr, np.uint32), np.zeros(nr), np.zeros(nv, np.uint32), np.zeros(nv)]
+    _lib.call("crest_matrix_qc", dm.handle, _lib.ptr(s["cm"]), _lib.ptr(s["gm"]), _lib.ptr(flag), nr, nv,
+              *[_lib.ptr(a) for a in out])
+
+
+@pytest.mark.parametrize("indexed", [False, True])
+@pytest.mark.parametrize("integral", [True, False])
+def test_extract_with_and_without_order_check(small_counts, indexed, integral):
+    """Strictly gene-sorted rows (known once the range index exists) skip the
+    column-order check; either way, and for non-integral values (the
+    entry-order normalisation total), the FP64 Gram equals the oracle's."""
+    s = setup(small_counts, 12)
+    data = s["data"] if integral else (s["data"] * np.float32(0.37)).astype(np.float32)
+    s = dict(s, data=data)
+    dm = DeviceMatrix(s["indptr"], s["indices"], data, s["n_genes"], "device", chunk_cells=400)
+    if indexed:
+        build_range_index(s, dm)
+    scale = _lib.Scale(1, _lib.ptr(s["mean"]), _lib.ptr(s["std"]), 10.0)
+    p = tl.PcaPlan(s["d"], "fp64")
+    p.accumulate(dm, s["cm"], s["gm"], 1e4, True, s["sub"], s["nv"], scale)
+    Go, co = oracle_gram(s)
+    iu = np.triu_indices(s["d"])
+    assert np.array_equal(p.gram()[iu], Go[iu])
+    assert np.array_equal(p.results()[3], co)
+    p.close()
+    dm.close()
+
+
+def test_duplicates_rejected_after_range_index(small_counts):
+    """A row holding a gene twice is sorted but not strictly: the range index
+    keeps the order check on and the duplicate is still rejected."""
+    s = setup(small_counts, 6)  # a seed that keeps cell 7, which holds the duplicate
+    ip2, ix2, dx2 = with_duplicate(s)
+    s2 = dict(s, indptr=ip2, indices=ix2, data=dx2)
+    dm = DeviceMatrix(ip2, ix2, dx2, s["n_genes"], "device", chunk_cells=400)
+    build_range_index(s2, dm)
+    scale = _lib.Scale(1, _lib.ptr(s["mean"]), _lib.ptr(s["std"]), 10.0)
+    p = tl.PcaPlan(s["d"], "fp64")
+    with pytest.raises(ValueError, match="twice"):
+        p.accumulate(dm, s["cm"], s["gm"], 1e4, True, s["sub"], s["nv"], scale)
+    p.close()
+    dm.close()
+
+
+def test_extract_wide_gene_table(small_counts):
+    """70,000 store genes: the int16 code table no longer leaves room for two
+    blocks per SM and the byte-class extract runs; the same FP64 Gram."""
+    indptr, indices, data = small_counts[:3]
+    s = setup((indptr, indices, data, 70_000), 14, d_frac=0.0)
+    # HVG columns among the stored genes (ids below 600)
+    rng = np.random.default_rng(14)
+    stored = np.flatnonzero(s["gm"][:600] >= 0)
+    pick = np.sort(rng.choice(stored, 150, replace=False))
+    sub = np.full(s["nv"], -1, np.int32)
+    sub[s["gm"][pick]] = np.arange(150, dtype=np.int32)
+    st = np.zeros((s["nv"], 5))
+    oracle.gene_stats(indices, data, s["cm"], s["gm"], 1e4, True, None, indptr, 0, st)
+    nk = s["nr"]
+    mean = st[:, 0] / nk
+    std = np.sqrt(np.maximum((st[:, 1] - nk * mean * mean) / (nk - 1), 0))
+    std[std == 0] = 1
+    mask = sub >= 0
+    s.update(d=150, sub=sub, mean=np.ascontiguousarray(mean[mask]), std=np.ascontiguousarray(std[mask]))
+    p, dm, _ = plan_gram(s, "device")
+    Go, co = oracle_gram(s)
+    iu = np.triu_indices(150)
+    assert np.array_equal(p.gram()[iu], Go[iu])
+    assert np.array_equal(p.results()[3], co)
+    p.close()
+    dm.close()
 
 
 def shuffled_rows(s, seed):
