@@ -63,7 +63,7 @@ struct GramBufs {
         w.shift = shift.as<double>();
         w.status = status.as<int>();
         w.gram_aux = nullptr;
-        w.colsum_rows = 3 * (int64_t)device_sms();
+        w.colsum_rows = 2 * (int64_t)device_sms();
         CREST_TRY(colsum_part.ensure(sizeof(long long) * (size_t)w.colsum_rows * (size_t)w.d_pad));
         w.colsum_part = colsum_part.as<long long>();
         if (precision == CREST_GRAM_BF16X3 && d > 0) {

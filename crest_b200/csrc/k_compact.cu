@@ -314,11 +314,8 @@ int launch_extract(const DevChunk &c, const uint32_t *cls, const int32_t *code, 
     if (c.n_spans == 0) return CREST_OK;
     CREST_REQUIRE(!c.span_cell, CREST_EINVAL, "extract needs CSR chunks");
     if (d < 32767) {  // the int16 codes exist (launch_hvg_code)
-        static const int depth = [] {  // blocks loading ahead (tuning; 1 or 2)
-            const char *e = getenv("CREST_EXTRACT_DEPTH");
-            return e && e[0] == '2' ? 2 : 1;
-        }();
-        const void *fn = depth == 2 ? (const void *)k_extract16<2> : (const void *)k_extract16<1>;
+        // one block loading ahead: two measured 4.58 against 4.49 ms at 1M cells
+        const void *fn = (const void *)k_extract16<1>;
         const size_t smem = 2 * (size_t)code16_slots(c.n_gene_map);
         int per_sm = 0;
         if (smem <= (size_t)kMaxSmem) {
@@ -328,14 +325,9 @@ int launch_extract(const DevChunk &c, const uint32_t *cls, const int32_t *code, 
         if (per_sm >= 2) {
             const int64_t blocks =
                 std::min<int64_t>(ceil_div(c.n_spans, kExtract16Warps), (int64_t)device_sms() * per_sm);
-            const int16_t *tab = codes16(code, c.n_gene_map);
             prof::Scope ps("extract_csr", st);
-            if (depth == 2)
-                k_extract16<2><<<(unsigned)blocks, kExtract16Warps * 32, smem, st>>>(c, tab, (int32_t)d,
-                                                                                     check_order ? 1 : 0, out);
-            else
-                k_extract16<1><<<(unsigned)blocks, kExtract16Warps * 32, smem, st>>>(c, tab, (int32_t)d,
-                                                                                     check_order ? 1 : 0, out);
+            k_extract16<1><<<(unsigned)blocks, kExtract16Warps * 32, smem, st>>>(c, codes16(code, c.n_gene_map),
+                                                                                 (int32_t)d, check_order ? 1 : 0, out);
             CREST_CUDA_TRY(cudaGetLastError());
             return CREST_OK;
         }
@@ -423,6 +415,10 @@ __global__ void __launch_bounds__(kDensifyCWarps * 32, MINB) k_densify_compact(
     // to the f64 global sum, so a tile's total (at most 2^13 cells) cannot
     // overflow.  Each block writes its row of partials; k_colsum_reduce adds
     // them up in block order.
+    // (Keeping each column's mean, std, bias and shift in shared memory
+    // instead of four L1 gathers per entry measured slower: 6.76 against
+    // 6.43 ms per 1M-cell step -- fewer long-scoreboard stalls, more
+    // shared-memory and barrier stalls.)
     long long *s_col = reinterpret_cast<long long *>(smem);
     E *shift_row = reinterpret_cast<E *>(smem + (priv ? sizeof(double) * (size_t)round_up(d, 2) : 0));
     if (priv) {
@@ -524,9 +520,9 @@ __global__ void k_colsum_reduce(const long long *__restrict__ part, int nb, int6
     }
 }
 
-// Resident blocks per SM and entry loads per lane in flight: two blocks of
-// 16 warps with eight loads each (64 registers), or three blocks with four
-// (40 registers; CREST_DENSIFY_OCC=3).
+// Two resident blocks of 16 warps per SM, eight entry loads per lane in
+// flight (64 registers).  Three blocks with four loads each (40 registers)
+// measured slower at 1M cells: 6.77 against 6.43 ms per step.
 template <int MODE, int MINB, int DU>
 static int densify_compact_t(const int64_t *indptr, int64_t cell0, int64_t n, const CompactHvg &in,
                              double target_sum, int log1p, const DevScale &t, const double *shift,
@@ -557,13 +553,6 @@ template <int MODE>
 static int densify_compact_t(const int64_t *indptr, int64_t cell0, int64_t n, const CompactHvg &in,
                              double target_sum, int log1p, const DevScale &t, const double *shift,
                              const GramWork &w, int64_t m_pad, cudaStream_t st, double *col_pass) {
-    static const bool occ3 = [] {
-        const char *e = getenv("CREST_DENSIFY_OCC");
-        return e && e[0] == '3';
-    }();
-    if (occ3)
-        return densify_compact_t<MODE, 3, 4>(indptr, cell0, n, in, target_sum, log1p, t, shift, w, m_pad, st,
-                                             col_pass);
     return densify_compact_t<MODE, 2, kDensifyU>(indptr, cell0, n, in, target_sum, log1p, t, shift, w, m_pad, st,
                                                  col_pass);
 }

@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(256) k_range_index(const int64_t *__restrict__
         uint32_t carry_g = 0;  // gene of the previous entry
         int carry_r = 0;       // its range (0 before the first entry)
         bool have_prev = false, bad = false, dup = false;
-        constexpr int U = 8;
+        constexpr int U = 16;  // 16 gene-id loads per lane in flight
         for (int64_t s = lo; s < hi; s += 32 * U) {
             uint32_t g[U];
 #pragma unroll
@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(256) k_cell_totals(DevChunk c, double *__restr
         span_row(c, i, lo, hi);
         uint64_t s = 0;  // exact while every kept value is an integer in [0, 2^24)
         bool ok = true;
-        for_entries_x4<true>(c, lo, hi, [&](uint32_t g) { return ((s_keep[g >> 5] >> (g & 31)) & 1u) ? 0 : -1; },
+        for_entries_x4<true, 2>(c, lo, hi, [&](uint32_t g) { return ((s_keep[g >> 5] >> (g & 31)) & 1u) ? 0 : -1; },
                              [&](const int32_t (&m)[4], const float (&x)[4]) {
 #pragma unroll
                                  for (int u = 0; u < 4; ++u) {
