@@ -740,7 +740,8 @@ int crest_pca_create(crest_pca **out, int64_t d, int32_t precision) {
     memset(&p->stats, 0, sizeof p->stats);
     int rc = zeros<double>(p->gram, d * d, 0);
     if (!rc) rc = zeros<double>(p->colsum, d, 0);
-    if (!rc) rc = p->gb.ensure(p->w, d, precision, tile_cells_default());
+    // a first tile; crest_pca_accumulate sizes it for the matrix it reads
+    if (!rc) rc = p->gb.ensure(p->w, d, precision, std::min<int64_t>(tile_cells_default(), 16384));
     if (!rc && cudaDeviceSynchronize() != cudaSuccess) {
         set_error("PCA plan set-up failed: %s", cudaGetErrorString(cudaGetLastError()));
         rc = CREST_ECUDA;
@@ -784,6 +785,11 @@ int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
     const DevChunk proto = base_chunk(m, target_sum, log1p);
     CREST_TRY(stage_hvg_code(proto, m->sub_map.as<int32_t>(), n_vars, p->d, m->code, st));
     CREST_TRY(gram_status_reset(p->w, st));
+    {  // tiles: up to one upload chunk of a resident matrix, one stored chunk of a streamed one
+        const int64_t cap = m->residency == CREST_MEM_DEVICE ? std::min<int64_t>(tile_cells_default(), kUploadCells)
+                                                               : std::min<int64_t>(tile_cells_default(), m->chunk_cells);
+        CREST_TRY(p->gb.ensure(p->w, p->d, p->precision, std::min(cap, round_up(std::max<int64_t>(m->n_cells, 1), 64))));
+    }
     bool compact = false;
     CREST_TRY(compact_pass(m, proto, p->d, compact, st));
     if (compact) m->cmp_packed = false;

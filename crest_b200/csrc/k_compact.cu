@@ -412,8 +412,8 @@ __global__ void __launch_bounds__(kDensifyCWarps * 32, MINB) k_densify_compact(
     // column sums of the stored entries' scaled values in 32.32 fixed point
     // (native 64-bit integer shared atomics; exact, so the block's partial
     // does not depend on the order of the adds); |s| >= 2^12 goes straight
-    // to the f64 global sum, so a tile's total (at most 2^13 cells) cannot
-    // overflow.  Each block writes its row of partials; k_colsum_reduce adds
+    // to the f64 global sum, so a block's total over a tile (at most 2^19
+    // cells) stays below 2^31 and cannot overflow.  Each block writes its row of partials; k_colsum_reduce adds
     // them up in block order.
     // (Keeping each column's mean, std, bias and shift in shared memory
     // instead of four L1 gathers per entry measured slower: 6.76 against
@@ -561,6 +561,8 @@ int launch_densify_compact(const int64_t *indptr, int64_t cell0, int64_t n, cons
                            int log1p, const DevScale &t, const GramWork &w, cudaStream_t st, double *colsum_pass,
                            bool shift_ready) {
     CREST_REQUIRE(n <= w.m_cap, CREST_EINVAL, "tile holds %lld cells, piece has %lld", (long long)w.m_cap,
+                  (long long)n);
+    CREST_REQUIRE(n <= ((int64_t)1 << 19), CREST_EINVAL, "a Gram tile holds at most 2^19 cells (got %lld)",
                   (long long)n);
     const int64_t m_pad = round_up(n > 0 ? n : 1, 64);
     CREST_CUDA_TRY(cudaMemsetAsync(w.n_kept, 0, 2 * sizeof(int64_t), st));

@@ -91,6 +91,24 @@ __global__ void __launch_bounds__(kCscThreads, 1)
     }
 }
 
+// Per store cell: target / total of its kept genes (1 without
+// normalisation, or when the total is 0), or -1 for a dropped cell -- one
+// 8-byte gather per entry in the gene-major pass instead of the cell map's
+// and the totals' (each entry of a sparse gene's column meets a new sector).
+__global__ void k_cell_scale(DevChunk c, int64_t n_cells, const double *__restrict__ total, double *__restrict__ cs) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_cells) return;
+    double v = -1.0;
+    if (i < c.n_cell_map && c.cell_map[i] >= 0) {
+        v = 1.0;
+        if (c.target_sum > 0.0) {
+            const double t = total[i];
+            v = t > 0.0 ? c.target_sum / t : 1.0;
+        }
+    }
+    cs[i] = v;
+}
+
 // Five sums of one segment of a gene's column per CTA: out[m * 5 + s] +=
 // (x, x^2, expm1 x, expm1(x)^2, 1) over the segment's entries of kept
 // cells, x the transformed value.
@@ -99,9 +117,8 @@ __global__ void __launch_bounds__(256) k_gene_stats_csc(DevChunk c, const int64_
                                                         const int64_t *__restrict__ col_ptr,
                                                         const uint32_t *__restrict__ col_cell,
                                                         const float *__restrict__ col_val,
-                                                        const double *__restrict__ total, double *__restrict__ out) {
+                                                        const double *__restrict__ cell_scale, double *__restrict__ out) {
     __shared__ double red[5][8];
-    const bool norm = c.target_sum > 0.0;
     for (int64_t s = blockIdx.x; s < n_segs; s += gridDim.x) {
         const int32_t g = seg_gene[s];
         const int32_t m = g < c.n_gene_map ? __ldg(c.gene_map + g) : -1;
@@ -112,12 +129,8 @@ __global__ void __launch_bounds__(256) k_gene_stats_csc(DevChunk c, const int64_
         for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
             const uint32_t cell = __ldcs(col_cell + e);
             const float x = __ldcs(col_val + e);
-            if ((int64_t)cell >= c.n_cell_map || __ldg(c.cell_map + cell) < 0) continue;
-            double scale = 1.0;
-            if (norm) {
-                const double t = __ldg(total + cell);
-                scale = t > 0.0 ? c.target_sum / t : 1.0;
-            }
+            const double scale = __ldg(cell_scale + cell);
+            if (scale < 0.0) continue;  // dropped cell
             const double v = (double)transform_value(c, scale, x);
             const double ev = expm1(v);
             a[0] += v;
@@ -194,13 +207,17 @@ int build_csc(const int64_t *indptr, const uint32_t *genes, const float *values,
     return CREST_OK;
 }
 
-int launch_gene_stats_csc(const DevChunk &c, const CscMatrix &m, const double *total, double *out, cudaStream_t st) {
+int launch_gene_stats_csc(const DevChunk &c, CscMatrix &m, const double *total, double *out, cudaStream_t st) {
     if (m.n_segs == 0) return CREST_OK;
+    CREST_TRY(m.cell_scale.ensure(8 * (size_t)std::max<int64_t>(c.n_spans, 1)));
     prof::Scope ps("gene_stats_csc", st);
+    if (c.n_spans)
+        k_cell_scale<<<(unsigned)ceil_div(c.n_spans, 256), 256, 0, st>>>(c, c.n_spans, total,
+                                                                          m.cell_scale.as<double>());
     const int64_t blocks = std::min<int64_t>(m.n_segs, (int64_t)device_sms() * 8);
     k_gene_stats_csc<<<(unsigned)blocks, 256, 0, st>>>(c, m.seg_lo.as<int64_t>(), m.seg_gene.as<int32_t>(), m.n_segs,
                                                         m.col_ptr.as<int64_t>(), m.col_cell.as<uint32_t>(),
-                                                        m.col_val.as<float>(), total, out);
+                                                        m.col_val.as<float>(), m.cell_scale.as<double>(), out);
     CREST_CUDA_TRY(cudaGetLastError());
     return CREST_OK;
 }

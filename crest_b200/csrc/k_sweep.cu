@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(256) k_range_index(const int64_t *__restrict__
         uint32_t carry_g = 0;  // gene of the previous entry
         int carry_r = 0;       // its range (0 before the first entry)
         bool have_prev = false, bad = false, dup = false;
-        constexpr int U = 16;  // 16 gene-id loads per lane in flight
+        constexpr int U = 8;
         for (int64_t s = lo; s < hi; s += 32 * U) {
             uint32_t g[U];
 #pragma unroll
@@ -213,6 +213,8 @@ __device__ __forceinline__ void cta_cells(int64_t n_spans, int64_t &c0, int64_t 
 // 32-bit integer shared-memory atomics without a return value are used (the
 // fast ones on this part); per-cell sums are integer lane sums.
 // status bit 1: a non-integral value was seen.
+constexpr int32_t kQcFlagBit = 1 << 30;  // kept gene indices stay below 2^30
+
 __global__ void __launch_bounds__(kSweepThreads, 1)
     k_qc_sweep(DevChunk c, RangeIndex ix, const uint8_t *__restrict__ flag, uint32_t *__restrict__ gene_ncells,
                double *__restrict__ gene_total, RowOut ro, int *status) {
@@ -221,12 +223,13 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
     uint32_t *s_lo = reinterpret_cast<uint32_t *>(smem);  // [S] sum of the low 16 bits
     uint32_t *s_hi = s_lo + S;                             // [S] sum of the high bits
     uint32_t *s_cnt = s_hi + S;                            // [S]
-    int32_t *s_map = reinterpret_cast<int32_t *>(s_cnt + S);  // [S] gene_map of the range
-    uint8_t *s_flag = reinterpret_cast<uint8_t *>(s_map + S);  // [S] flag of the mapped gene
+    // [S] gene_map of the range with the flag of the mapped gene in bit 30
+    // (-1: dropped), one shared-memory read per entry for both
+    int32_t *s_map = reinterpret_cast<int32_t *>(s_cnt + S);
     int64_t c0, c1;
     cta_cells(c.n_spans, c0, c1);
     const int64_t nc = c1 - c0;
-    double *s_t = reinterpret_cast<double *>(s_flag + S);    // [nc]
+    double *s_t = reinterpret_cast<double *>(s_map + S);     // [nc]
     double *s_f = s_t + nc;                                   // [nc]
     uint32_t *s_n = reinterpret_cast<uint32_t *>(s_f + nc);  // [nc]
     const int lane = lane_id();
@@ -247,8 +250,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
         for (int i = threadIdx.x; i < S; i += blockDim.x) {
             const int64_t g = (int64_t)g0 + i;
             const int32_t m = g < c.n_gene_map ? __ldg(c.gene_map + g) : -1;
-            s_map[i] = m;
-            s_flag[i] = m >= 0 ? flag[m] : 0;
+            s_map[i] = m >= 0 && flag[m] ? (m | kQcFlagBit) : m;
         }
         __syncthreads();
         uint64_t ts = 0, fs = 0;
@@ -268,7 +270,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
                 non_integral = non_integral || !ok;
                 const uint32_t xi = ok ? (uint32_t)x : 0u;
                 ts += xi;
-                if (s_flag[j]) fs += xi;
+                if (m & kQcFlagBit) fs += xi;
                 n += 1;
                 atomicAdd(s_cnt + j, 1u);
                 atomicAdd(s_lo + j, xi & 0xffffu);
@@ -288,7 +290,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
         for (int i = threadIdx.x; i < S; i += blockDim.x) {
             const uint32_t k = s_cnt[i];
             if (k) {
-                const int32_t m = s_map[i];  // counted entries have m >= 0
+                const int32_t m = s_map[i] & ~kQcFlagBit;  // counted entries have a mapped gene
                 atomicAdd(gene_ncells + m, k);
                 atomicAdd(gene_total + m, (double)(((uint64_t)s_hi[i] << 16) + s_lo[i]));
                 s_cnt[i] = 0u;
@@ -392,7 +394,7 @@ __global__ void __launch_bounds__(256) k_cell_totals(DevChunk c, double *__restr
         span_row(c, i, lo, hi);
         uint64_t s = 0;  // exact while every kept value is an integer in [0, 2^24)
         bool ok = true;
-        for_entries_x4<true, 2>(c, lo, hi, [&](uint32_t g) { return ((s_keep[g >> 5] >> (g & 31)) & 1u) ? 0 : -1; },
+        for_entries_x4<true>(c, lo, hi, [&](uint32_t g) { return ((s_keep[g >> 5] >> (g & 31)) & 1u) ? 0 : -1; },
                              [&](const int32_t (&m)[4], const float (&x)[4]) {
 #pragma unroll
                                  for (int u = 0; u < 4; ++u) {
@@ -425,7 +427,7 @@ int launch_range_index(const int64_t *indptr, const uint32_t *genes, int64_t n_c
 }
 
 size_t qc_sweep_smem(int log2_s, int64_t cells_per_cta) {
-    return (size_t)(1 << log2_s) * 17 + (size_t)cells_per_cta * 20;
+    return (size_t)(1 << log2_s) * 16 + (size_t)cells_per_cta * 20;
 }
 
 int sweep_ctas(int64_t n_spans, int64_t cell_cap) {
@@ -438,7 +440,8 @@ int sweep_ctas(int64_t n_spans, int64_t cell_cap) {
 int launch_qc_sweep(const DevChunk &c, const RangeIndex &ix, const uint8_t *flag, uint32_t *gene_ncells,
                     double *gene_total, const RowOut &row, int *status, cudaStream_t st) {
     if (c.n_spans == 0) return CREST_OK;
-    const int64_t cap = std::min<int64_t>(((int64_t)kMaxSmem - (int64_t)(1 << ix.log2_s) * 17) / 20, 65536);
+    CREST_REQUIRE(c.n_gene_map < kQcFlagBit, CREST_EINVAL, "QC sweep: at most 2^30 genes");
+    const int64_t cap = std::min<int64_t>(((int64_t)kMaxSmem - (int64_t)(1 << ix.log2_s) * 16) / 20, 65536);
     const int ctas = sweep_ctas(c.n_spans, cap);
     const size_t smem = qc_sweep_smem(ix.log2_s, ceil_div(c.n_spans, ctas));
     CREST_REQUIRE(smem <= (size_t)kMaxSmem, CREST_EINVAL, "QC sweep: %zu B of shared memory", smem);

@@ -30,9 +30,10 @@ int launch_gene_stats(const DevChunk &c, double *out, cudaStream_t st);
 // of at most 16384 entries of one gene start at seg_lo[s] (gene seg_gene[s]).
 struct CscMatrix {
     DevBuf col_ptr, col_cell, col_val, seg_lo, seg_gene;
+    DevBuf cell_scale;  // per store cell: its normalisation factor, or -1 when dropped
     int64_t n_segs = 0, n_genes = 0;
     void release() {
-        for (auto *b : {&col_ptr, &col_cell, &col_val, &seg_lo, &seg_gene}) b->release();
+        for (auto *b : {&col_ptr, &col_cell, &col_val, &seg_lo, &seg_gene, &cell_scale}) b->release();
         n_segs = n_genes = 0;
     }
 };
@@ -40,7 +41,7 @@ int build_csc(const int64_t *indptr, const uint32_t *genes, const float *values,
               int64_t nnz, CscMatrix &out, cudaStream_t st);
 // gene_stats of a whole matrix (c: the matrix as one chunk, for its maps and
 // transform) from its gene-major copy, given the per-cell kept-gene totals.
-int launch_gene_stats_csc(const DevChunk &c, const CscMatrix &m, const double *total, double *out, cudaStream_t st);
+int launch_gene_stats_csc(const DevChunk &c, CscMatrix &m, const double *total, double *out, cudaStream_t st);
 
 // Exact k nearest neighbours (self excluded) of the rows of X (n x d f32, device).
 int launch_knn(const float *X, int64_t n, int d, int k, uint32_t *idx, float *dist, cudaStream_t st);
