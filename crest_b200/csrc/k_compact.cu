@@ -3,8 +3,9 @@
 // The Gram pass (src/kernels.rs:227-309) and the projection pass (:352-371)
 // both need, per cell, the normalisation total over kept genes and the
 // cell's HVG entries in entry order; only about one stored entry in eight
-// is an HVG entry.  k_extract streams the CSR once (16-byte loads, one warp
-// per cell, a 2-bit kept/HVG class per store gene in shared memory): it adds
+// is an HVG entry.  k_extract16 streams the CSR once (16-byte loads, one
+// warp per cell, the int16 code of every store gene in shared memory; the
+// byte-class k_extract where that table does not fit): it adds
 // up the kept values and writes the HVG entries (column, raw value) into the
 // cell's slot of a compact array laid out like the CSR (slot of cell i =
 // [indptr[i], indptr[i+1]), filled from the front), with the entry count and
@@ -14,10 +15,12 @@
 //
 // Duplicate (cell, column) entries: the reference's pairwise loop gives
 // v1^2 + v1 v2 + v2^2 on the diagonal for two entries of one gene, which a
-// dense tile cannot represent.  k_extract checks that every cell's HVG
-// columns are strictly increasing (true for gene-sorted rows and a monotone
-// column map); when some cell is not, k_dup_compact looks for a real
-// duplicate with a per-warp bit set and the Gram pass reports an error.
+// dense tile cannot represent.  The extract kernels check that every
+// cell's HVG columns are strictly increasing (true for gene-sorted rows and a
+// monotone column map; the check is skipped when the matrix's range index
+// has shown every row strictly sorted and the column map is monotone); when
+// some cell is not, k_dup_compact looks for a real duplicate with a per-warp
+// bit set and the Gram pass reports an error.
 #include <cuda_bf16.h>
 
 #include "kernels.cuh"

@@ -156,7 +156,8 @@ struct CompactHvg {
     double *scale;   // [n_cells]
     int *status;     // bit 0: some cell's columns not strictly increasing; bit 1: a duplicate column
 };
-// 2-bit kept / HVG class per store gene from the code table (words of 16 genes).
+// Kept / HVG class byte per store gene from the code table (for the byte-class
+// extract kernel; words of four genes, a multiple of four words).
 size_t gene_class_words(int64_t n_gene_map);
 int launch_gene_class(const int32_t *code, int64_t n_gene_map, int64_t d, uint32_t *cls, cudaStream_t st);
 // One read of a whole CSR matrix (c.base == 0, CSR spans) into the compact form.
