@@ -449,6 +449,10 @@ def main_gpu(args):
     if "extract_csr" in table:  # one CSR read per step, in launches of one upload chunk each
         n_l, tot, mx = table["extract_csr"]
         hbm["extract_csr"] = bytes_pass / (tot / max(1, args.steps) / 1e3) / 1e9
+    if "densify" in table:  # the bf16 hi/lo tile rows written per step (compact-form reads not counted)
+        n_l, tot, mx = table["densify"]
+        d_pad = -(-P["d"] // 256) * 256
+        hbm["densify_tile"] = n_rows * d_pad * 4 / (tot / max(1, args.steps) / 1e3) / 1e9
     extra["hbm_gbs"] = hbm
     extra["hbm_frac"] = {kk: v / peaks["hbm_gbs"] for kk, v in hbm.items()}
 
