@@ -48,6 +48,9 @@ struct crest_matrix {
     int range_log2_s = 12, n_ranges = 0;
     crest::DevBuf range_off, status;
     int qc_integral = 1;  // cleared once the QC sweep meets a non-integral value
+    // set once a QC sweep with every store gene mapped met only integers in
+    // [0, 2^24): every stored value is then a small non-negative integer
+    bool values_small_int = false;
     // per-cell kept-gene totals of a device-resident matrix for the gene_map
     // they were formed with
     crest::DevBuf totals;
@@ -397,7 +400,8 @@ int compact_extract(crest_matrix *m, const DevChunk &proto, int64_t d, int64_t c
     c.first_cell = (uint32_t)c0;
     c.base = 0;
     c.n_spans = c1 - c0;
-    return launch_extract(c, m->cls.as<uint32_t>(), m->code.as<int32_t>(), d, compact_view(m), check_order, st);
+    return launch_extract(c, m->cls.as<uint32_t>(), m->code.as<int32_t>(), d, compact_view(m), check_order, st,
+                          m->values_small_int);
 }
 
 // True when the HVG column of a store gene (sub_map[gene_map[g]], as
@@ -617,6 +621,10 @@ int crest_matrix_qc(crest_matrix *m, const int64_t *cell_map, const int32_t *gen
         int status = 0;
         CREST_CUDA_TRY(cudaMemcpyAsync(&status, m->status.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
         CREST_CUDA_TRY(cudaStreamSynchronize(st));
+        // the sweep visits the mapped cells' entries of mapped genes only
+        if (!status && std::all_of(gene_map, gene_map + m->n_genes, [](int32_t g) { return g >= 0; }) &&
+            std::all_of(cell_map, cell_map + m->n_cells, [](int64_t r) { return r >= 0; }))
+            m->values_small_int = true;
         if (status) {  // a non-integral value: redo in entry order
             m->qc_integral = 0;
             swept = false;

@@ -175,7 +175,8 @@ __device__ __noinline__ double kept_total_ordered16(const DevChunk &c, int64_t l
 
 template <int DEPTH>
 __global__ void __launch_bounds__(kExtract16Warps * 32, 3)
-    k_extract16(DevChunk c, const int16_t *__restrict__ code16, int32_t d, int check_order, CompactHvg out) {
+    k_extract16(DevChunk c, const int16_t *__restrict__ code16, int32_t d, int check_order, int known_int,
+                CompactHvg out) {
     extern __shared__ __align__(16) int16_t s_code[];
     {
         const int64_t n_words = code16_slots(c.n_gene_map) / 8, n_src = round_up(c.n_gene_map, 8) / 8;
@@ -218,7 +219,7 @@ __global__ void __launch_bounds__(kExtract16Warps * 32, 3)
                 if (norm) {
                     const float xk = v[u] >= 0 ? x[u] : 0.0f;
                     fsum += xk;
-                    bad |= __float_as_uint(xk - rintf(xk)) | (__float_as_uint(xk) & 0x80000000u);
+                    if (!known_int) bad |= __float_as_uint(xk - rintf(xk)) | (__float_as_uint(xk) & 0x80000000u);
                 }
                 hv[u] = (uint32_t)v[u] < (uint32_t)d;
                 const unsigned bal = __ballot_sync(kFull, hv[u]);
@@ -313,7 +314,7 @@ __global__ void __launch_bounds__(kExtract16Warps * 32, 3)
 }
 
 int launch_extract(const DevChunk &c, const uint32_t *cls, const int32_t *code, int64_t d, const CompactHvg &out,
-                   bool check_order, cudaStream_t st) {
+                   bool check_order, cudaStream_t st, bool known_int) {
     if (c.n_spans == 0) return CREST_OK;
     CREST_REQUIRE(!c.span_cell, CREST_EINVAL, "extract needs CSR chunks");
     if (d < 32767) {  // the int16 codes exist (launch_hvg_code)
@@ -329,8 +330,8 @@ int launch_extract(const DevChunk &c, const uint32_t *cls, const int32_t *code, 
             const int64_t blocks =
                 std::min<int64_t>(ceil_div(c.n_spans, kExtract16Warps), (int64_t)device_sms() * per_sm);
             prof::Scope ps("extract_csr", st);
-            k_extract16<1><<<(unsigned)blocks, kExtract16Warps * 32, smem, st>>>(c, codes16(code, c.n_gene_map),
-                                                                                 (int32_t)d, check_order ? 1 : 0, out);
+            k_extract16<1><<<(unsigned)blocks, kExtract16Warps * 32, smem, st>>>(
+                c, codes16(code, c.n_gene_map), (int32_t)d, check_order ? 1 : 0, known_int ? 1 : 0, out);
             CREST_CUDA_TRY(cudaGetLastError());
             return CREST_OK;
         }

@@ -164,8 +164,10 @@ int launch_gene_class(const int32_t *code, int64_t n_gene_map, int64_t d, uint32
 // check_order = false when every row is known to be strictly gene-sorted and
 // the HVG columns increase with the gene id (the columns of every cell are
 // then strictly increasing and need no check).
+// known_int: every stored value is known to be an integer in [0, 2^24)
+// (the per-entry integrality test of the kept totals is then skipped).
 int launch_extract(const DevChunk &c, const uint32_t *cls, const int32_t *code, int64_t d, const CompactHvg &out,
-                   bool check_order, cudaStream_t st);
+                   bool check_order, cudaStream_t st, bool known_int = false);
 // Exact duplicate-column check of every cell (sets bit 1 of *in.status).
 int launch_dup_compact(const int64_t *indptr, int64_t n_cells, const CompactHvg &in, int64_t d, cudaStream_t st);
 // Densify cells [cell0, cell0 + n) of the compact form into the Gram tile.

@@ -104,28 +104,36 @@ def oracle_gram(s, indices=None, data=None, indptr=None):
     return Go, co
 
 
-def build_range_index(s, dm):
+def build_range_index(s, dm, all_mapped=False):
     """A QC pass over a device matrix builds its gene-range index, which also
-    records whether every row is strictly sorted by gene."""
-    nr, nv = s["nr"], s["nv"]
+    records whether every row is strictly sorted by gene.  With every cell
+    and gene mapped it also learns whether all stored values are small
+    non-negative integers (the extract then skips its per-entry test)."""
+    if all_mapped:
+        n, g = len(s["indptr"]) - 1, s["n_genes"]
+        cm, gm, nr, nv = np.arange(n, dtype=np.int64), np.arange(g, dtype=np.int32), n, g
+    else:
+        cm, gm, nr, nv = s["cm"], s["gm"], s["nr"], s["nv"]
     flag = np.zeros(nv, np.bool_)
     out = [np.zeros(nr), np.zeros(nr, np.uint32), np.zeros(nr), np.zeros(nv, np.uint32), np.zeros(nv)]
-    _lib.call("crest_matrix_qc", dm.handle, _lib.ptr(s["cm"]), _lib.ptr(s["gm"]), _lib.ptr(flag), nr, nv,
+    _lib.call("crest_matrix_qc", dm.handle, _lib.ptr(cm), _lib.ptr(gm), _lib.ptr(flag), nr, nv,
               *[_lib.ptr(a) for a in out])
 
 
-@pytest.mark.parametrize("indexed", [False, True])
+@pytest.mark.parametrize("indexed", [False, True, "all"])
 @pytest.mark.parametrize("integral", [True, False])
 def test_extract_with_and_without_order_check(small_counts, indexed, integral):
     """Strictly gene-sorted rows (known once the range index exists) skip the
-    column-order check; either way, and for non-integral values (the
-    entry-order normalisation total), the FP64 Gram equals the oracle's."""
+    column-order check, and a QC over every cell and gene that met only small
+    integers lets the extract skip its per-entry integrality test; in every
+    case, and for non-integral values (the entry-order normalisation total),
+    the FP64 Gram equals the oracle's."""
     s = setup(small_counts, 12)
     data = s["data"] if integral else (s["data"] * np.float32(0.37)).astype(np.float32)
     s = dict(s, data=data)
     dm = DeviceMatrix(s["indptr"], s["indices"], data, s["n_genes"], "device", chunk_cells=400)
     if indexed:
-        build_range_index(s, dm)
+        build_range_index(s, dm, all_mapped=indexed == "all")
     scale = _lib.Scale(1, _lib.ptr(s["mean"]), _lib.ptr(s["std"]), 10.0)
     p = tl.PcaPlan(s["d"], "fp64")
     p.accumulate(dm, s["cm"], s["gm"], 1e4, True, s["sub"], s["nv"], scale)
