@@ -587,7 +587,7 @@ def main_gpu(args):
                 "vs_baseline": None, "dtype": "bf16x3", "data": "synthetic",
                 "config": {"workload": workload_label(wl, n_gen), "gram": "split-BF16 (bf16x3) tcgen05",
                            "cells_after_qc": n_rows, "nnz": nnz, "hvg": P["d"], "l2": l2_note,
-                           "gram_tile_cells": int(os.environ.get("CREST_TILE_CELLS", 131072)),
+                           "gram_tile_cells": min(int(os.environ.get("CREST_TILE_CELLS", 262144)), n_rows),
                            "parallelism": f"dp{ws}" if ws > 1 else "1 GPU"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "e2e_streamed": e2e_streamed,
                 "gpu_launches": launches, "clocks": clocks,

@@ -793,8 +793,13 @@ int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
     const DevChunk proto = base_chunk(m, target_sum, log1p);
     CREST_TRY(stage_hvg_code(proto, m->sub_map.as<int32_t>(), n_vars, p->d, m->code, st));
     CREST_TRY(gram_status_reset(p->w, st));
-    {  // tiles: up to one upload chunk of a resident matrix, one stored chunk of a streamed one
-        const int64_t cap = m->residency == CREST_MEM_DEVICE ? std::min<int64_t>(tile_cells_default(), kUploadCells)
+    // a resident matrix already on the device is one range of tiles; while its
+    // upload is in flight the tiles follow the upload chunks
+    const bool resident = m->residency == CREST_MEM_DEVICE && m->up_waited;
+    {  // tiles: the default size for a resident matrix, at most one upload chunk while
+       // uploading, one stored chunk of a streamed matrix
+        const int64_t cap = resident ? tile_cells_default()
+                            : m->residency == CREST_MEM_DEVICE ? std::min<int64_t>(tile_cells_default(), kUploadCells)
                                                                : std::min<int64_t>(tile_cells_default(), m->chunk_cells);
         CREST_TRY(p->gb.ensure(p->w, p->d, p->precision, std::min(cap, round_up(std::max<int64_t>(m->n_cells, 1), 64))));
     }
@@ -811,8 +816,9 @@ int crest_pca_accumulate(crest_pca *p, crest_matrix *m, const int64_t *cell_map,
         // monotone column map give strictly increasing columns in every cell
         const bool check_order = !(m->rows_strict && columns_monotone(gene_map, m->n_genes, sub_map, n_vars));
         int64_t u0 = 0;
-        for (size_t u = 0; u < m->up_end.size() && u0 < m->n_cells; ++u) {
-            const int64_t u1 = m->up_end[u];
+        const size_t n_ranges = resident ? 1 : m->up_end.size();
+        for (size_t u = 0; u < n_ranges && u0 < m->n_cells; ++u) {
+            const int64_t u1 = resident ? m->n_cells : m->up_end[u];
             if (!m->up_waited) {
                 CREST_TRY(issue_uploads(m, u + 2));  // keep the next chunk's copy queued
                 CREST_CUDA_TRY(cudaStreamWaitEvent(st, m->up_ev[u], 0));

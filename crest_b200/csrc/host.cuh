@@ -38,11 +38,12 @@ inline int zeros(DevBuf &b, int64_t n, cudaStream_t st) {
 // tiles amortise the SYRK's prologue and its FP64 read-modify-write of the
 // Gram, and the densify's tail.  At 1M cells (bf16x3, d = 2000) the step
 // measured 50.2 / 43.0 / 42.1 / 41.2 ms with 8,192 / 32,768 / 65,536 /
-// 131,072-cell tiles at the same accuracy (max angle 0.006 deg to FP64).
-// At most 2^19 (the densify's fixed-point column sums).
+// 131,072-cell tiles at the same accuracy (max angle 0.006 deg to FP64),
+// and 40.0 ms (0.0065 deg) with 262,144-cell tiles over the whole resident
+// matrix.  At most 2^19 (the densify's fixed-point column sums).
 inline int64_t tile_cells_default() {
     const char *e = getenv("CREST_TILE_CELLS");
-    int64_t v = e ? atoll(e) : 131072;
+    int64_t v = e ? atoll(e) : 262144;
     if (v < 64) v = 64;
     if (v > ((int64_t)1 << 19)) v = (int64_t)1 << 19;
     return round_up(v, 64);
