@@ -96,6 +96,27 @@ def test_compact_projection_equals_csr_projection(small_counts, k):
         x.close()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+def test_many_tiles_during_and_after_the_upload(small_counts, monkeypatch, precision):
+    """256-cell Gram tiles: the first pass tiles the cells as their upload
+    chunk arrives, a later pass tiles the resident matrix as one range; both
+    give the same Gram, and the FP64 form the oracle's bit for bit."""
+    monkeypatch.setenv("CREST_TILE_CELLS", "256")
+    s = setup(small_counts, 15)
+    p, dm, scale = plan_gram(s, "device", precision)
+    G1, c1 = p.gram().copy(), p.results()[3].copy()
+    p.reset()
+    p.accumulate(dm, s["cm"], s["gm"], 1e4, True, s["sub"], s["nv"], scale)
+    G2, c2 = p.gram(), p.results()[3]
+    iu = np.triu_indices(s["d"])
+    assert np.array_equal(G1[iu], G2[iu]) and np.array_equal(c1, c2)
+    if precision == "fp64":
+        Go, co = oracle_gram(s)
+        assert np.array_equal(G2[iu], Go[iu]) and np.array_equal(c2, co)
+    p.close()
+    dm.close()
+
+
 def oracle_gram(s, indices=None, data=None, indptr=None):
     Go, co = np.zeros((s["d"], s["d"])), np.zeros(s["d"])
     oracle.gram_accumulate(s["indices"] if indices is None else indices, s["data"] if data is None else data,
