@@ -653,7 +653,7 @@ int crest_project(const crest_chunk *chunk, const int32_t *sub_map, int64_t n_va
     CREST_TRY(launch_project(dc, x->code.as<int32_t>(), d, ds, x->loadings.as<double>(), (int)k,
                              x->out3.as<float>(), 1, x->counter.as<unsigned int>(), st));
     std::vector<float> part(s.n * k);
-    if (s.n * k)
+    if (!part.empty())
         CREST_CUDA_TRY(cudaMemcpyAsync(part.data(), x->out3.ptr, 4 * s.n * k, cudaMemcpyDeviceToHost, st));
     CREST_CUDA_TRY(cudaStreamSynchronize(st));
     for (int64_t i = 0; i < s.n; ++i) {

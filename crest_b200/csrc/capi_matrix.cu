@@ -954,7 +954,7 @@ int crest_pca_project(crest_pca *p, crest_matrix *m, const int64_t *cell_map, co
         CREST_TRY(p->xbuf.ensure(4 * (size_t)std::max<int64_t>(n_rows * p->k, 1)));
         X = p->xbuf.as<float>();
     }
-    if (n_rows * p->k)
+    if (n_rows > 0 && p->k > 0)
         k_fill_scores<<<(unsigned)ceil_div(n_rows * p->k, 256), 256, 0, st>>>(p->shift.as<double>(), n_rows, p->k, X);
     CREST_CUDA_TRY(cudaGetLastError());
     const DevChunk proto = base_chunk(m, target_sum, log1p);
@@ -970,7 +970,7 @@ int crest_pca_project(crest_pca *p, crest_matrix *m, const int64_t *cell_map, co
                                   m->counter.as<unsigned int>(), st);
         }));
     }
-    if (out_mem != CREST_MEM_DEVICE && n_rows * p->k)
+    if (out_mem != CREST_MEM_DEVICE && n_rows > 0 && p->k > 0)
         CREST_CUDA_TRY(cudaMemcpyAsync(out, X, 4 * (size_t)(n_rows * p->k), cudaMemcpyDeviceToHost, st));
     p->stats.project_ms = t.stop();
     CREST_CUDA_TRY(cudaGetLastError());
